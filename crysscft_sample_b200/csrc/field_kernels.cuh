@@ -1,0 +1,232 @@
+// Field kernels of one SCFT iteration (FP64 fields; contour slices of type T).
+//
+//  prep    : calc_ksi (src/crysSCFT_sample.cpp:341-346), array_exp (:315-322) for the
+//            two Boltzmann factors, and the initial slices q(0) = 1, q+(end) = 1 (:483)
+//  Q       : array_average of q+_A(0) (:324-331, :494)
+//  phi     : integrate_phi, trapezoid weights (:348-360), both blocks
+//  energy  : the sums of print_energy (:398-424) and the max incompressibility
+//  update  : calc_new_fields, simple mixing (:362-371)
+//
+// Reductions are deterministic: a fixed grid writes per-block partials, the last
+// block to finish (atomic ticket, no waiting) reduces them in a fixed order.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace crysscft {
+
+constexpr int kRedThreads = 256;
+constexpr int kRedMaxBlocks = 592;  // 4 x 148 SMs
+
+// Layout of the per-iteration record written by energy_kernel (doubles).
+enum { HIST_F = 0, HIST_EH, HIST_E0, HIST_E1, HIST_EK, HIST_MAXINC, HIST_Q, HIST_FLAGS, HIST_STRIDE };
+
+struct IterState {
+    double Q;            // partition function of the current iteration
+    unsigned ticket_q;   // last-block tickets
+    unsigned ticket_e;
+    unsigned iteration;  // iterations completed since the counter was reset
+    int error;           // bit 0: Q <= 0 or not finite, bit 1: F not finite
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    return v;
+}
+// block-wide sum / max over kRedThreads threads; result valid in thread 0
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (w == 0) {
+        r = lane < (kRedThreads / 32) ? sh[lane] : 0.0;
+        r = warp_sum(r);
+    }
+    return r;
+}
+__device__ __forceinline__ double block_max(double v, double* sh) {
+    v = warp_max(v);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (w == 0) {
+        r = lane < (kRedThreads / 32) ? sh[lane] : 0.0;
+        r = warp_max(r);
+    }
+    return r;
+}
+
+template <typename T>
+__global__ void prep_kernel(const double* __restrict__ wA, const double* __restrict__ wB,
+                            double* __restrict__ ksi, T* __restrict__ wAds, T* __restrict__ wBds,
+                            T* __restrict__ q_first, T* __restrict__ qc_last, double xN, double ds,
+                            long long M) {
+    const double index = -ds / 2;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < M;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double a = wA[i], b = wB[i];
+        ksi[i] = 0.5 * (a + b - xN);
+        wAds[i] = (T)(1. * exp(index * a));
+        wBds[i] = (T)(1. * exp(index * b));
+        q_first[i] = T(1);
+        qc_last[i] = T(1);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads)
+q_reduce_kernel(const T* __restrict__ qc0, long long M, double* __restrict__ partials,
+                IterState* st) {
+    __shared__ double sh[kRedThreads / 32];
+    __shared__ bool last;
+    double s = 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < M;
+         i += (long long)gridDim.x * blockDim.x)
+        s += (double)qc0[i];
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) {
+        partials[blockIdx.x] = s;
+        __threadfence();
+        const unsigned t = atomicAdd(&st->ticket_q, 1u);
+        last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double r = 0.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) r += __ldcg(&partials[i]);
+    r = block_sum(r, sh);
+    if (threadIdx.x == 0) {
+        const double Q = r / (double)M;
+        st->Q = Q;
+        st->ticket_q = 0;
+        if (!(Q > 0.0) || !isfinite(Q)) st->error |= 1;
+    }
+}
+
+// phi_A = sum_{u=0}^{NsA} w_u fA/(NsA Q) q[u] q+[u];  phi_B over u = NsA..NsA+NsB.
+// q (forward chain) and qc (backward chain) hold U+1 = NsA+NsB+1 slices of M.
+template <typename T>
+__global__ void phi_kernel(const T* __restrict__ q, const T* __restrict__ qc, double* __restrict__ phiA,
+                           double* __restrict__ phiB, const IterState* st, double fA, long long NsA,
+                           long long NsB, long long M) {
+    const double Q = st->Q;
+    const double fB = 1 - fA;
+    const double cA = fA / (NsA * Q);
+    const double cB = fB / (NsB * Q);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < M;
+         i += (long long)gridDim.x * blockDim.x) {
+        double a = 0.0;
+        for (long long s = 0; s <= NsA; ++s) {
+            double factor = s == 0 ? 0.5 : (s == NsA ? 0.5 : 1);
+            factor *= cA;
+            a += factor * (double)q[s * M + i] * (double)qc[s * M + i];
+        }
+        double b = 0.0;
+        for (long long s = 0; s <= NsB; ++s) {
+            double factor = s == 0 ? 0.5 : (s == NsB ? 0.5 : 1);
+            factor *= cB;
+            const long long u = NsA + s;
+            b += factor * (double)q[u * M + i] * (double)qc[u * M + i];
+        }
+        phiA[i] = a;
+        phiB[i] = b;
+    }
+}
+
+__global__ void __launch_bounds__(kRedThreads)
+energy_kernel(const double* __restrict__ wA, const double* __restrict__ wB,
+              const double* __restrict__ phiA, const double* __restrict__ phiB,
+              const double* __restrict__ ksi, double xN, long long M, double* __restrict__ partials,
+              IterState* st, double* __restrict__ hist, unsigned hist_cap) {
+    __shared__ double sh[kRedThreads / 32];
+    __shared__ bool last;
+    double e1 = 0.0, eh = 0.0, ek = 0.0, mx = 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < M;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double pa = phiA[i], pb = phiB[i];
+        e1 += -wA[i] * pa - wB[i] * pb;
+        eh += xN * pa * pb;
+        const double temp = 1 - pa - pb;
+        ek += -ksi[i] * temp;
+        mx = fmax(mx, fabs(temp));
+    }
+    e1 = block_sum(e1, sh);
+    eh = block_sum(eh, sh);
+    ek = block_sum(ek, sh);
+    mx = block_max(mx, sh);
+    if (threadIdx.x == 0) {
+        partials[4 * blockIdx.x + 0] = e1;
+        partials[4 * blockIdx.x + 1] = eh;
+        partials[4 * blockIdx.x + 2] = ek;
+        partials[4 * blockIdx.x + 3] = mx;
+        __threadfence();
+        const unsigned t = atomicAdd(&st->ticket_e, 1u);
+        last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double r1 = 0.0, rh = 0.0, rk = 0.0, rm = 0.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
+        r1 += __ldcg(&partials[4 * i + 0]);
+        rh += __ldcg(&partials[4 * i + 1]);
+        rk += __ldcg(&partials[4 * i + 2]);
+        rm = fmax(rm, __ldcg(&partials[4 * i + 3]));
+    }
+    r1 = block_sum(r1, sh);
+    rh = block_sum(rh, sh);
+    rk = block_sum(rk, sh);
+    rm = block_max(rm, sh);
+    if (threadIdx.x == 0) {
+        const double Q = st->Q;
+        const double fe_entropic_0 = -log(Q);
+        const double fe_entropic_1 = r1 / (double)M;
+        const double fe_enthalpic = rh / (double)M;
+        const double fe_ksi = rk / (double)M;
+        const double F = fe_entropic_0 + fe_entropic_1 + fe_enthalpic + fe_ksi;
+        if (!isfinite(F)) st->error |= 2;
+        double* h = hist + (size_t)(st->iteration % hist_cap) * HIST_STRIDE;
+        h[HIST_F] = F;
+        h[HIST_EH] = fe_enthalpic;
+        h[HIST_E0] = fe_entropic_0;
+        h[HIST_E1] = fe_entropic_1;
+        h[HIST_EK] = fe_ksi;
+        h[HIST_MAXINC] = rm;
+        h[HIST_Q] = Q;
+        h[HIST_FLAGS] = (double)st->error;
+        st->ticket_e = 0;
+    }
+}
+
+__global__ void update_kernel(double* __restrict__ wA, double* __restrict__ wB,
+                              const double* __restrict__ phiA, const double* __restrict__ phiB,
+                              const double* __restrict__ ksi, double xN, double acc, long long M,
+                              IterState* st) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < M;
+         i += (long long)gridDim.x * blockDim.x) {
+        wA[i] += acc * (xN * phiB[i] + ksi[i] - wA[i]);
+        wB[i] += acc * (xN * phiA[i] + ksi[i] - wB[i]);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->iteration += 1;
+}
+
+// dst[i] = src[i] (type conversion allowed)
+template <typename D, typename S>
+__global__ void convert_kernel(D* __restrict__ dst, const S* __restrict__ src, long long M) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < M;
+         i += (long long)gridDim.x * blockDim.x)
+        dst[i] = (D)src[i];
+}
+
+}  // namespace crysscft

@@ -1,0 +1,686 @@
+// C ABI of the B200 propagator library (see include/crysscft_b200.h).
+//
+// Host side: solver objects holding the per-axis operators (built once per
+// (cell, ds) in long double, stored FP64 and FP32 on the device), the
+// triplet/contour launchers, and the AB-diblock iteration context whose whole
+// iteration is captured once into a CUDA graph and replayed.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/crysscft_b200.h"
+#include "axis_kernels.cuh"
+#include "field_kernels.cuh"
+#include "operators.h"
+
+using namespace crysscft;
+
+namespace {
+
+thread_local std::string g_last_error = "";
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+#define CK(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(e_ == cudaErrorMemoryAllocation ? SCFT_ERR_ALLOC : SCFT_ERR_CUDA, \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));              \
+    } while (0)
+
+#define CKR(call)                          \
+    do {                                   \
+        int r_ = (call);                   \
+        if (r_ != SCFT_OK) return r_;      \
+    } while (0)
+
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    int alloc(size_t count) {
+        release();
+        if (count == 0) return SCFT_OK;
+        cudaError_t e = cudaMalloc((void**)&p, count * sizeof(T));
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return fail(SCFT_ERR_ALLOC, std::string("cudaMalloc(") + std::to_string(count * sizeof(T)) +
+                                            " bytes): " + cudaGetErrorString(e));
+        }
+        n = count;
+        return SCFT_OK;
+    }
+};
+
+struct OpsSet {
+    DevBuf<double> d_op[3], d_opT[3];
+    DevBuf<float> f_op[3], f_opT[3];
+};
+
+int upload_operator(const std::vector<long double>& A, int n, OpsSet& s, int axis) {
+    std::vector<double> d((size_t)n * n), dt((size_t)n * n);
+    std::vector<float> f((size_t)n * n), ft((size_t)n * n);
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) {
+            const long double v = A[(size_t)i * n + j];
+            d[(size_t)i * n + j] = (double)v;
+            dt[(size_t)j * n + i] = (double)v;
+            f[(size_t)i * n + j] = (float)v;
+            ft[(size_t)j * n + i] = (float)v;
+        }
+    const size_t nn = (size_t)n * n;
+    CKR(s.d_op[axis].alloc(nn));
+    CKR(s.d_opT[axis].alloc(nn));
+    CKR(s.f_op[axis].alloc(nn));
+    CKR(s.f_opT[axis].alloc(nn));
+    CK(cudaMemcpy(s.d_op[axis].p, d.data(), nn * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(s.d_opT[axis].p, dt.data(), nn * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(s.f_op[axis].p, f.data(), nn * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(s.f_opT[axis].p, ft.data(), nn * sizeof(float), cudaMemcpyHostToDevice));
+    return SCFT_OK;
+}
+
+int grid_blocks(long long M, int threads) {
+    long long b = (M + threads - 1) / threads;
+    if (b > 148LL * 8) b = 148LL * 8;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
+// ---------------------------------------------------------------------------
+// axis-pass launchers
+// ---------------------------------------------------------------------------
+template <typename T, int BM>
+cudaError_t launch_strided_bm(const AxisPass<T>& p, int nchain, cudaStream_t st) {
+    constexpr int BN = 64, BK = 16, TM = 4, TN = 4;
+    dim3 grid((unsigned)((p.inner + BN - 1) / BN), (unsigned)((p.n + BM - 1) / BM),
+              (unsigned)(p.outer * nchain));
+    axis_strided_kernel<T, BM, BN, BK, TM, TN><<<grid, (BM / TM) * (BN / TN), 0, st>>>(p);
+    return cudaGetLastError();
+}
+template <typename T, int BN>
+cudaError_t launch_contig_bn(const AxisPass<T>& p, int nchain, cudaStream_t st) {
+    constexpr int BM = 64, BK = 16, TM = 4, TN = 4;
+    dim3 grid((unsigned)((p.n + BN - 1) / BN), (unsigned)((p.outer + BM - 1) / BM), (unsigned)nchain);
+    axis_contig_kernel<T, BM, BN, BK, TM, TN><<<grid, (BM / TM) * (BN / TN), 0, st>>>(p);
+    return cudaGetLastError();
+}
+template <typename T>
+cudaError_t launch_axis(const AxisPass<T>& p, int nchain, bool contiguous, cudaStream_t st) {
+    if (contiguous) {
+        if (p.n <= 16) return launch_contig_bn<T, 16>(p, nchain, st);
+        if (p.n <= 32) return launch_contig_bn<T, 32>(p, nchain, st);
+        return launch_contig_bn<T, 64>(p, nchain, st);
+    }
+    if (p.n <= 16) return launch_strided_bm<T, 16>(p, nchain, st);
+    if (p.n <= 32) return launch_strided_bm<T, 32>(p, nchain, st);
+    return launch_strided_bm<T, 64>(p, nchain, st);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// solver
+// ---------------------------------------------------------------------------
+struct scft_solver_s {
+    int kind = 0;
+    int precision = SCFT_FP64;
+    int device = 0;
+    size_t grid_log[3] = {0, 0, 0};
+    size_t grid_phy[3] = {0, 0, 0};
+    size_t M = 0;
+    double cell[6] = {4, 4, 4, 0, 0, 0};  // src/solver_base.h:43 default
+    double ds = 0.0;
+    bool ds_set = false;
+    std::map<double, std::unique_ptr<OpsSet>> ops_cache;  // per ds, cleared by set_cell_para
+    OpsSet* ops = nullptr;
+    unsigned long long ops_gen = 0;  // bumped whenever `ops` may point elsewhere
+    cudaStream_t stream = nullptr;
+    double* iomat = nullptr;  // pinned host buffer (get_iomat_for_diffusion)
+    DevBuf<double> d_io, d_t1, d_t2;
+    DevBuf<float> f_io, f_t1, f_t2, f_pre;
+    size_t launches = 0;
+
+    ~scft_solver_s() {
+        if (iomat) cudaFreeHost(iomat);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    int build_ops(double ds_) {
+        auto s = std::make_unique<OpsSet>();
+        for (int ax = 0; ax < 3; ++ax) {
+            std::vector<long double> A;
+            const int N = (int)grid_log[ax];
+            if (kind == SCFT_SOLVER_PMMM)
+                A = pmmm_axis_operator(N / 2, (long double)cell[0], (long double)ds_);
+            else if (kind == SCFT_SOLVER_P1)
+                A = p1_axis_operator(N, (long double)cell[ax], (long double)ds_);
+            else
+                A = m3_axis_operator(N, (long double)cell[ax], (long double)ds_);
+            CKR(upload_operator(A, (int)grid_phy[ax], *s, ax));
+        }
+        ops = s.get();
+        ops_cache[ds_] = std::move(s);
+        ++ops_gen;
+        return SCFT_OK;
+    }
+
+    // one triplet per chain: in -> (pre) z-pass -> t1 -> y-pass -> t2 -> x-pass (post) -> out
+    template <typename T>
+    int triplet(int nchain, const ChainIO<T> io[2], T* t1[2], T* t2[2], cudaStream_t st) {
+        const int nx = (int)grid_phy[0], ny = (int)grid_phy[1], nz = (int)grid_phy[2];
+        const T* opx;
+        const T* opy;
+        const T* opz;
+        const T* opxT;
+        const T* opyT;
+        const T* opzT;
+        if constexpr (sizeof(T) == 8) {
+            opx = (const T*)ops->d_op[0].p; opy = (const T*)ops->d_op[1].p; opz = (const T*)ops->d_op[2].p;
+            opxT = (const T*)ops->d_opT[0].p; opyT = (const T*)ops->d_opT[1].p; opzT = (const T*)ops->d_opT[2].p;
+        } else {
+            opx = (const T*)ops->f_op[0].p; opy = (const T*)ops->f_op[1].p; opz = (const T*)ops->f_op[2].p;
+            opxT = (const T*)ops->f_opT[0].p; opyT = (const T*)ops->f_opT[1].p; opzT = (const T*)ops->f_opT[2].p;
+        }
+        AxisPass<T> pz{}, py{}, px{};
+        for (int c = 0; c < nchain; ++c) {
+            pz.ch[c] = ChainIO<T>{io[c].in, t1[c], io[c].pre, nullptr};
+            py.ch[c] = ChainIO<T>{t1[c], t2[c], nullptr, nullptr};
+            px.ch[c] = ChainIO<T>{t2[c], io[c].out, nullptr, io[c].post};
+        }
+        pz.op = opz; pz.opT = opzT; pz.n = nz; pz.outer = (long long)nx * ny; pz.inner = 1;
+        py.op = opy; py.opT = opyT; py.n = ny; py.outer = nx; py.inner = nz;
+        px.op = opx; px.opT = opxT; px.n = nx; px.outer = 1; px.inner = (long long)ny * nz;
+        CK(launch_axis(pz, nchain, true, st));
+        CK(launch_axis(py, nchain, false, st));
+        CK(launch_axis(px, nchain, false, st));
+        launches += 3;
+        return SCFT_OK;
+    }
+};
+
+struct scft_diblock_s {
+    scft_solver_t solver = nullptr;
+    double fA = 0, ds = 0, xN = 0, acc = 0;
+    size_t NsA = 0, NsB = 0, U = 0, M = 0;
+    int precision = SCFT_FP64;
+    bool fields_set = false;
+    DevBuf<double> wA, wB, phiA, phiB, ksi, partials, hist;
+    DevBuf<double> d_wAds, d_wBds, d_q, d_qc, d_t[4];
+    DevBuf<float> f_wAds, f_wBds, f_q, f_qc, f_t[4];
+    DevBuf<IterState> state;
+    unsigned hist_cap = 1024;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    size_t launches_per_iter = 0;
+    unsigned long long captured_gen = ~0ULL;
+
+    ~scft_diblock_s() {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        if (graph) cudaGraphDestroy(graph);
+    }
+
+    template <typename T>
+    int enqueue_iteration(cudaStream_t st, T* wAds, T* wBds, T* q, T* qc, T** t) {
+        const long long MM = (long long)M;
+        const int blocks = grid_blocks(MM, 256);
+        size_t launches = 0;
+        prep_kernel<T><<<blocks, 256, 0, st>>>(wA.p, wB.p, ksi.p, wAds, wBds, q, qc + U * M, xN, ds, MM);
+        CK(cudaGetLastError());
+        ++launches;
+        const size_t before = solver->launches;
+        for (size_t t_ = 0; t_ < U; ++t_) {
+            // forward chain: q[t] -> q[t+1] with block A (t < NsA) or B
+            // backward chain: qc[U-t] -> qc[U-t-1] with the block of segment U-t-1
+            const T* w1 = t_ < NsA ? wAds : wBds;
+            const size_t ub = U - t_ - 1;
+            const T* w2 = ub < NsA ? wAds : wBds;
+            ChainIO<T> io[2];
+            io[0] = ChainIO<T>{q + t_ * M, q + (t_ + 1) * M, w1, w1};
+            io[1] = ChainIO<T>{qc + (ub + 1) * M, qc + ub * M, w2, w2};
+            T* t1[2] = {t[0], t[1]};
+            T* t2[2] = {t[2], t[3]};
+            CKR(solver->triplet<T>(2, io, t1, t2, st));
+        }
+        launches += solver->launches - before;
+        const int rblocks = (int)std::min<long long>(kRedMaxBlocks, (MM + kRedThreads - 1) / kRedThreads);
+        q_reduce_kernel<T><<<rblocks, kRedThreads, 0, st>>>(qc, MM, partials.p, state.p);
+        CK(cudaGetLastError());
+        phi_kernel<T><<<blocks, 256, 0, st>>>(q, qc, phiA.p, phiB.p, state.p, fA, (long long)NsA,
+                                              (long long)NsB, MM);
+        CK(cudaGetLastError());
+        energy_kernel<<<rblocks, kRedThreads, 0, st>>>(wA.p, wB.p, phiA.p, phiB.p, ksi.p, xN, MM,
+                                                       partials.p, state.p, hist.p, hist_cap);
+        CK(cudaGetLastError());
+        update_kernel<<<blocks, 256, 0, st>>>(wA.p, wB.p, phiA.p, phiB.p, ksi.p, xN, acc, MM, state.p);
+        CK(cudaGetLastError());
+        launches += 4;
+        launches_per_iter = launches;
+        return SCFT_OK;
+    }
+
+    int enqueue(cudaStream_t st) {
+        if (precision == SCFT_FP64) {
+            double* t[4] = {d_t[0].p, d_t[1].p, d_t[2].p, d_t[3].p};
+            return enqueue_iteration<double>(st, d_wAds.p, d_wBds.p, d_q.p, d_qc.p, t);
+        }
+        float* t[4] = {f_t[0].p, f_t[1].p, f_t[2].p, f_t[3].p};
+        return enqueue_iteration<float>(st, f_wAds.p, f_wBds.p, f_q.p, f_qc.p, t);
+    }
+
+    int ensure_graph() {
+        if (gexec) return SCFT_OK;
+        cudaStream_t st = solver->stream;
+        CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        int r = enqueue(st);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(st, &g);
+        if (r != SCFT_OK) {
+            if (g) cudaGraphDestroy(g);
+            return r;
+        }
+        if (e != cudaSuccess) return fail(SCFT_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+        graph = g;
+        CK(cudaGraphInstantiate(&gexec, graph, 0));
+        return SCFT_OK;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* scft_last_error(void) { return g_last_error.c_str(); }
+
+const char* scft_status_string(int s) {
+    switch (s) {
+        case SCFT_OK: return "SCFT_OK";
+        case SCFT_ERR_INVALID_ARG: return "SCFT_ERR_INVALID_ARG";
+        case SCFT_ERR_BAD_GRID: return "SCFT_ERR_BAD_GRID";
+        case SCFT_ERR_CUDA: return "SCFT_ERR_CUDA";
+        case SCFT_ERR_ALLOC: return "SCFT_ERR_ALLOC";
+        case SCFT_ERR_NOT_READY: return "SCFT_ERR_NOT_READY";
+        case SCFT_ERR_NUMERIC: return "SCFT_ERR_NUMERIC";
+        case SCFT_ERR_TIMEOUT: return "SCFT_ERR_TIMEOUT";
+        case SCFT_ERR_UNSUPPORTED: return "SCFT_ERR_UNSUPPORTED";
+        case SCFT_ERR_NO_DEVICE: return "SCFT_ERR_NO_DEVICE";
+        default: return "SCFT_ERR_UNKNOWN";
+    }
+}
+
+const char* scft_version(void) { return "crysscft_b200 0.1 (sm_100a)"; }
+
+int scft_solver_create(int kind, const size_t grid_size_log[3], const double translational_part[9],
+                       int precision, int device, scft_solver_t* out) {
+    if (!out || !grid_size_log) return fail(SCFT_ERR_INVALID_ARG, "null argument");
+    *out = nullptr;
+    if (kind < SCFT_SOLVER_P1 || kind > SCFT_SOLVER_PMMM) return fail(SCFT_ERR_INVALID_ARG, "bad solver kind");
+    if (precision != SCFT_FP64 && precision != SCFT_FP32) return fail(SCFT_ERR_INVALID_ARG, "bad precision");
+    const size_t Nx = grid_size_log[0], Ny = grid_size_log[1], Nz = grid_size_log[2];
+    // grid checks of the reference constructors (src/solver_p1.h:101-108,
+    // src/solver_3m.h:81-92, src/solver_Pmmm.h:71-82); the GPU path has no alignment rule
+    if (Nx == 0 || Ny == 0 || Nz == 0) return fail(SCFT_ERR_BAD_GRID, "ERROR: Bad Grid Size");
+    if (kind != SCFT_SOLVER_P1 && (Nx % 2 || Ny % 2 || Nz % 2))
+        return fail(SCFT_ERR_BAD_GRID, "ERROR: Grid Size Must Be Even For this symmetry");
+    const size_t maxn = 1024;
+    if (Nx > maxn || Ny > maxn || Nz > maxn) return fail(SCFT_ERR_BAD_GRID, "grid too large");
+    if (kind == SCFT_SOLVER_3M && translational_part)
+        for (int i = 0; i < 9; ++i)
+            if (translational_part[i] != 0.0)
+                return fail(SCFT_ERR_UNSUPPORTED, "3m solver: non-zero mirror translations are not supported yet");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(SCFT_ERR_NO_DEVICE, "no CUDA device");
+    if (device < 0) CK(cudaGetDevice(&device));
+    if (device >= ndev) return fail(SCFT_ERR_INVALID_ARG, "bad device ordinal");
+    CK(cudaSetDevice(device));
+    auto s = std::make_unique<scft_solver_s>();
+    s->kind = kind;
+    s->precision = precision;
+    s->device = device;
+    for (int i = 0; i < 3; ++i) {
+        s->grid_log[i] = grid_size_log[i];
+        s->grid_phy[i] = kind == SCFT_SOLVER_P1 ? grid_size_log[i] : grid_size_log[i] / 2;
+    }
+    s->M = s->grid_phy[0] * s->grid_phy[1] * s->grid_phy[2];
+    CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    cudaError_t e = cudaHostAlloc((void**)&s->iomat, s->M * sizeof(double), cudaHostAllocDefault);
+    if (e != cudaSuccess) return fail(SCFT_ERR_ALLOC, "cudaHostAlloc iomat");
+    std::memset(s->iomat, 0, s->M * sizeof(double));
+    *out = s.release();
+    return SCFT_OK;
+}
+
+int scft_solver_destroy(scft_solver_t s) {
+    if (!s) return SCFT_OK;
+    cudaSetDevice(s->device);
+    cudaStreamSynchronize(s->stream);
+    delete s;
+    return SCFT_OK;
+}
+
+int scft_solver_set_cell_para(scft_solver_t s, const double c[6]) {
+    if (!s || !c) return fail(SCFT_ERR_INVALID_ARG, "null argument");
+    for (int i = 0; i < 3; ++i)
+        if (!(c[i] > 0.0) || !std::isfinite(c[i])) return fail(SCFT_ERR_INVALID_ARG, "cell lengths must be > 0");
+    if (s->kind == SCFT_SOLVER_PMMM) {
+        // src/solver_Pmmm.h:98-104: cubic, only cell_para[0] is used
+        const double c6[6] = {c[0], c[0], c[0], 0, 0, 0};
+        std::memcpy(s->cell, c6, sizeof(c6));
+    } else {
+        const double c6[6] = {c[0], c[1], c[2], 0, 0, 0};
+        std::memcpy(s->cell, c6, sizeof(c6));
+    }
+    CK(cudaSetDevice(s->device));
+    CK(cudaStreamSynchronize(s->stream));
+    s->ops_cache.clear();
+    s->ops = nullptr;
+    ++s->ops_gen;
+    s->ds = 0.0;
+    s->ds_set = false;
+    return SCFT_OK;
+}
+
+int scft_solver_set_contour_step(scft_solver_t s, double ds) {
+    if (!s) return fail(SCFT_ERR_INVALID_ARG, "null handle");
+    if (!(ds > 0.0) || !std::isfinite(ds)) return fail(SCFT_ERR_INVALID_ARG, "ds must be > 0");
+    CK(cudaSetDevice(s->device));
+    s->ds = ds;
+    s->ds_set = true;
+    auto it = s->ops_cache.find(ds);
+    if (it != s->ops_cache.end()) {
+        if (s->ops != it->second.get()) ++s->ops_gen;
+        s->ops = it->second.get();
+        return SCFT_OK;
+    }
+    return s->build_ops(ds);
+}
+
+int scft_solver_get_grid_size_log(scft_solver_t s, size_t out[3]) {
+    if (!s || !out) return fail(SCFT_ERR_INVALID_ARG, "null argument");
+    for (int i = 0; i < 3; ++i) out[i] = s->grid_log[i];
+    return SCFT_OK;
+}
+int scft_solver_get_grid_size_phy(scft_solver_t s, size_t out[3]) {
+    if (!s || !out) return fail(SCFT_ERR_INVALID_ARG, "null argument");
+    for (int i = 0; i < 3; ++i) out[i] = s->grid_phy[i];
+    return SCFT_OK;
+}
+int scft_solver_get_space_size_phy(scft_solver_t s, size_t* out) {
+    if (!s || !out) return fail(SCFT_ERR_INVALID_ARG, "null argument");
+    *out = s->M;
+    return SCFT_OK;
+}
+int scft_solver_get_cell_para(scft_solver_t s, double out[6]) {
+    if (!s || !out) return fail(SCFT_ERR_INVALID_ARG, "null argument");
+    std::memcpy(out, s->cell, sizeof(s->cell));
+    return SCFT_OK;
+}
+int scft_solver_get_ds(scft_solver_t s, double* out) {
+    if (!s || !out) return fail(SCFT_ERR_INVALID_ARG, "null argument");
+    *out = s->ds;
+    return SCFT_OK;
+}
+int scft_solver_get_iomat_for_diffusion(scft_solver_t s, double** out) {
+    if (!s || !out) return fail(SCFT_ERR_INVALID_ARG, "null argument");
+    *out = s->iomat;
+    return SCFT_OK;
+}
+
+static int solver_ready(scft_solver_t s) {
+    if (!s) return fail(SCFT_ERR_INVALID_ARG, "null handle");
+    if (!s->ds_set || !s->ops) return fail(SCFT_ERR_NOT_READY, "set_cell_para/set_contour_step first");
+    return SCFT_OK;
+}
+
+static int ensure_work(scft_solver_t s) {
+    if (s->d_t1.n != s->M) {
+        CKR(s->d_io.alloc(s->M));
+        CKR(s->d_t1.alloc(s->M));
+        CKR(s->d_t2.alloc(s->M));
+    }
+    return SCFT_OK;
+}
+
+int scft_solver_diffusion_device(scft_solver_t s, double* d_io, void* stream) {
+    CKR(solver_ready(s));
+    if (!d_io) return fail(SCFT_ERR_INVALID_ARG, "null buffer");
+    CK(cudaSetDevice(s->device));
+    CKR(ensure_work(s));
+    cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
+    ChainIO<double> io[2] = {{d_io, d_io, nullptr, nullptr}, {}};
+    // the z pass reads d_io into t1, the x pass writes d_io from t2: no aliasing inside a pass
+    double* t1[2] = {s->d_t1.p, nullptr};
+    double* t2[2] = {s->d_t2.p, nullptr};
+    return s->triplet<double>(1, io, t1, t2, st);
+}
+
+int scft_solver_diffusion(scft_solver_t s) {
+    CKR(solver_ready(s));
+    CK(cudaSetDevice(s->device));
+    CKR(ensure_work(s));
+    const size_t bytes = s->M * sizeof(double);
+    CK(cudaMemcpyAsync(s->d_io.p, s->iomat, bytes, cudaMemcpyHostToDevice, s->stream));
+    CKR(scft_solver_diffusion_device(s, s->d_io.p, s->stream));
+    CK(cudaMemcpyAsync(s->iomat, s->d_io.p, bytes, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return SCFT_OK;
+}
+
+int scft_solver_propagate_device(scft_solver_t s, double* d_q, const double* d_init,
+                                 const double* d_wds, size_t Ns, int direction, void* stream) {
+    CKR(solver_ready(s));
+    if (!d_q || !d_init || !d_wds) return fail(SCFT_ERR_INVALID_ARG, "null buffer");
+    if (direction != 1 && direction != -1) return fail(SCFT_ERR_INVALID_ARG, "Wrong direction");
+    CK(cudaSetDevice(s->device));
+    CKR(ensure_work(s));
+    cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
+    const size_t M = s->M;
+    size_t slot = direction == 1 ? 0 : Ns;
+    CK(cudaMemcpyAsync(d_q + slot * M, d_init, M * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    for (size_t k = 0; k < Ns; ++k) {
+        const size_t next = direction == 1 ? slot + 1 : slot - 1;
+        ChainIO<double> io[2] = {{d_q + slot * M, d_q + next * M, d_wds, d_wds}, {}};
+        double* t1[2] = {s->d_t1.p, nullptr};
+        double* t2[2] = {s->d_t2.p, nullptr};
+        CKR(s->triplet<double>(1, io, t1, t2, st));
+        slot = next;
+    }
+    return SCFT_OK;
+}
+
+int scft_solver_propagate(scft_solver_t s, double* q, const double* init, const double* wds, size_t Ns,
+                          int direction) {
+    CKR(solver_ready(s));
+    if (!q || !init || !wds) return fail(SCFT_ERR_INVALID_ARG, "null buffer");
+    CK(cudaSetDevice(s->device));
+    const size_t M = s->M;
+    DevBuf<double> dq, di, dw;
+    CKR(dq.alloc((Ns + 1) * M));
+    CKR(di.alloc(M));
+    CKR(dw.alloc(M));
+    CK(cudaMemcpyAsync(di.p, init, M * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    CK(cudaMemcpyAsync(dw.p, wds, M * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    CKR(scft_solver_propagate_device(s, dq.p, di.p, dw.p, Ns, direction, s->stream));
+    CK(cudaMemcpyAsync(q, dq.p, (Ns + 1) * M * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return SCFT_OK;
+}
+
+// ------------------------------- diblock ----------------------------------
+int scft_diblock_create(scft_solver_t s, double fA, double ds, double xN, double acceptance,
+                        scft_diblock_t* out) {
+    if (!s || !out) return fail(SCFT_ERR_INVALID_ARG, "null argument");
+    *out = nullptr;
+    if (!(fA > 0.0 && fA < 1.0)) return fail(SCFT_ERR_INVALID_ARG, "fA must be in (0,1)");
+    if (!(ds > 0.0)) return fail(SCFT_ERR_INVALID_ARG, "ds must be > 0");
+    // src/crysSCFT_sample.cpp:442-444 (truncating conversions)
+    const double fB = 1 - fA;
+    const size_t NsA = (size_t)(fA / ds);
+    const size_t NsB = (size_t)(fB / ds);
+    if (NsA < 1 || NsB < 1) return fail(SCFT_ERR_INVALID_ARG, "both blocks need at least one contour step");
+    CK(cudaSetDevice(s->device));
+    CKR(scft_solver_set_contour_step(s, ds));
+    auto d = std::make_unique<scft_diblock_s>();
+    d->solver = s;
+    d->fA = fA; d->ds = ds; d->xN = xN; d->acc = acceptance;
+    d->NsA = NsA; d->NsB = NsB; d->U = NsA + NsB; d->M = s->M;
+    d->precision = s->precision;
+    const size_t M = s->M;
+    CKR(d->wA.alloc(M)); CKR(d->wB.alloc(M)); CKR(d->phiA.alloc(M)); CKR(d->phiB.alloc(M));
+    CKR(d->ksi.alloc(M));
+    CKR(d->partials.alloc(4 * kRedMaxBlocks));
+    CKR(d->hist.alloc((size_t)d->hist_cap * HIST_STRIDE));
+    CKR(d->state.alloc(1));
+    CK(cudaMemset(d->state.p, 0, sizeof(IterState)));
+    CK(cudaMemset(d->phiA.p, 0, M * sizeof(double)));
+    CK(cudaMemset(d->phiB.p, 0, M * sizeof(double)));
+    if (d->precision == SCFT_FP64) {
+        CKR(d->d_wAds.alloc(M)); CKR(d->d_wBds.alloc(M));
+        CKR(d->d_q.alloc((d->U + 1) * M)); CKR(d->d_qc.alloc((d->U + 1) * M));
+        for (int i = 0; i < 4; ++i) CKR(d->d_t[i].alloc(M));
+    } else {
+        CKR(d->f_wAds.alloc(M)); CKR(d->f_wBds.alloc(M));
+        CKR(d->f_q.alloc((d->U + 1) * M)); CKR(d->f_qc.alloc((d->U + 1) * M));
+        for (int i = 0; i < 4; ++i) CKR(d->f_t[i].alloc(M));
+    }
+    *out = d.release();
+    return SCFT_OK;
+}
+
+int scft_diblock_destroy(scft_diblock_t d) {
+    if (!d) return SCFT_OK;
+    cudaSetDevice(d->solver->device);
+    cudaStreamSynchronize(d->solver->stream);
+    delete d;
+    return SCFT_OK;
+}
+
+int scft_diblock_get_contour_counts(scft_diblock_t d, size_t* NsA, size_t* NsB) {
+    if (!d) return fail(SCFT_ERR_INVALID_ARG, "null handle");
+    if (NsA) *NsA = d->NsA;
+    if (NsB) *NsB = d->NsB;
+    return SCFT_OK;
+}
+
+int scft_diblock_set_fields(scft_diblock_t d, const double* wA, const double* wB) {
+    if (!d || !wA || !wB) return fail(SCFT_ERR_INVALID_ARG, "null argument");
+    CK(cudaSetDevice(d->solver->device));
+    cudaStream_t st = d->solver->stream;
+    CK(cudaMemcpyAsync(d->wA.p, wA, d->M * sizeof(double), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d->wB.p, wB, d->M * sizeof(double), cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    d->fields_set = true;
+    return SCFT_OK;
+}
+
+int scft_diblock_get_fields(scft_diblock_t d, double* phiA, double* phiB, double* wA, double* wB) {
+    if (!d) return fail(SCFT_ERR_INVALID_ARG, "null handle");
+    CK(cudaSetDevice(d->solver->device));
+    cudaStream_t st = d->solver->stream;
+    const size_t b = d->M * sizeof(double);
+    if (phiA) CK(cudaMemcpyAsync(phiA, d->phiA.p, b, cudaMemcpyDeviceToHost, st));
+    if (phiB) CK(cudaMemcpyAsync(phiB, d->phiB.p, b, cudaMemcpyDeviceToHost, st));
+    if (wA) CK(cudaMemcpyAsync(wA, d->wA.p, b, cudaMemcpyDeviceToHost, st));
+    if (wB) CK(cudaMemcpyAsync(wB, d->wB.p, b, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return SCFT_OK;
+}
+
+int scft_diblock_device_fields(scft_diblock_t d, double** phiA, double** phiB, double** wA, double** wB) {
+    if (!d) return fail(SCFT_ERR_INVALID_ARG, "null handle");
+    if (phiA) *phiA = d->phiA.p;
+    if (phiB) *phiB = d->phiB.p;
+    if (wA) *wA = d->wA.p;
+    if (wB) *wB = d->wB.p;
+    d->fields_set = true;  // a caller that asks for device pointers may write the fields itself
+    return SCFT_OK;
+}
+
+static int diblock_run(scft_diblock_t d, size_t n_iter, double* F, double* parts, double* maxinc,
+                       double* Q) {
+    cudaStream_t st = d->solver->stream;
+    if (!d->solver->ds_set || !d->solver->ops || d->solver->ds != d->ds)
+        CKR(scft_solver_set_contour_step(d->solver, d->ds));
+    if (d->gexec && d->captured_gen != d->solver->ops_gen) {
+        cudaGraphExecDestroy(d->gexec);
+        cudaGraphDestroy(d->graph);
+        d->gexec = nullptr;
+        d->graph = nullptr;
+    }
+    CKR(d->ensure_graph());
+    d->captured_gen = d->solver->ops_gen;
+    size_t done = 0;
+    std::vector<double> h;
+    while (done < n_iter) {
+        const size_t chunk = std::min<size_t>(n_iter - done, d->hist_cap);
+        IterState zero{};
+        CK(cudaMemcpyAsync(d->state.p, &zero, sizeof(IterState), cudaMemcpyHostToDevice, st));
+        for (size_t i = 0; i < chunk; ++i) CK(cudaGraphLaunch(d->gexec, st));
+        h.resize(chunk * HIST_STRIDE);
+        CK(cudaMemcpyAsync(h.data(), d->hist.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        bool bad = false;
+        for (size_t i = 0; i < chunk; ++i) {
+            const double* r = &h[i * HIST_STRIDE];
+            if (F) F[done + i] = r[HIST_F];
+            if (parts) {
+                parts[4 * (done + i) + 0] = r[HIST_EH];
+                parts[4 * (done + i) + 1] = r[HIST_E0];
+                parts[4 * (done + i) + 2] = r[HIST_E1];
+                parts[4 * (done + i) + 3] = r[HIST_EK];
+            }
+            if (maxinc) maxinc[done + i] = r[HIST_MAXINC];
+            if (Q) Q[done + i] = r[HIST_Q];
+            if (r[HIST_FLAGS] != 0.0) bad = true;
+        }
+        done += chunk;
+        if (bad) return fail(SCFT_ERR_NUMERIC, "Q <= 0 or a non-finite free energy in an iteration");
+    }
+    return SCFT_OK;
+}
+
+int scft_diblock_iterate(scft_diblock_t d, size_t n_iter, double* F, double* parts, double* maxinc,
+                         double* Q) {
+    if (!d) return fail(SCFT_ERR_INVALID_ARG, "null handle");
+    if (!d->fields_set) return fail(SCFT_ERR_NOT_READY, "set_fields first");
+    CK(cudaSetDevice(d->solver->device));
+    return diblock_run(d, n_iter, F, parts, maxinc, Q);
+}
+
+int scft_diblock_iterate_host(scft_diblock_t d, double* wA, double* wB, size_t n_iter, double* phiA,
+                              double* phiB, double* F, double* parts, double* maxinc, double* Q) {
+    if (!d || !wA || !wB) return fail(SCFT_ERR_INVALID_ARG, "null argument");
+    CK(cudaSetDevice(d->solver->device));
+    CKR(scft_diblock_set_fields(d, wA, wB));
+    CKR(diblock_run(d, n_iter, F, parts, maxinc, Q));
+    return scft_diblock_get_fields(d, phiA, phiB, wA, wB);
+}
+
+int scft_diblock_launches_per_iteration(scft_diblock_t d, size_t* out) {
+    if (!d || !out) return fail(SCFT_ERR_INVALID_ARG, "null argument");
+    *out = d->launches_per_iter;
+    return SCFT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,110 @@
+"""Seeded synthetic initial fields (the reference reads BCC_fields_test.txt, which is not
+available, src/crysSCFT_sample.cpp:196).
+
+w_A = +A S(r) + noise_A, w_B = -A S(r) + noise_B with
+  BCC: S = cx cy + cy cz + cz cx,   FCC: S = cx cy cz,   c. = cos(2 pi . / L),
+sampled at x_i = (i + 1/2) L/N, so that every field is mirror-symmetric between grid
+points (f[i] = f[N-1-i] on each axis) and valid for all three solvers.  The
+Gaussian noise (sigma) is drawn on the first octant only and mirrored.
+
+Random numbers: a counter-based generator (SplitMix64 finaliser applied to
+seed ^ stream ^ counter) and the Box-Muller transform, so the fields are
+identical on every platform and numpy version.
+
+Layout helpers follow main()'s conventions (src/crysSCFT_sample.cpp:202-258):
+P1 uses the full grid, 3M the even sub-lattice f[2i,2j,2k], PMMM the first octant.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+_M64 = np.uint64(0xFFFFFFFFFFFFFFFF)
+
+
+def _splitmix64(x: np.ndarray) -> np.ndarray:
+    with np.errstate(over="ignore"):
+        z = x + np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return z ^ (z >> np.uint64(31))
+
+
+def uniform53(seed: int, stream: int, n: int) -> np.ndarray:
+    """n doubles in [0, 1) from (seed, stream, counter)."""
+    with np.errstate(over="ignore"):
+        key = _splitmix64(np.array([(seed * 0x100000001B3 + stream) & 0xFFFFFFFFFFFFFFFF], dtype=np.uint64))[0]
+        ctr = np.arange(n, dtype=np.uint64) * np.uint64(0xD1B54A32D192ED03)
+        bits = _splitmix64(ctr ^ key)
+    return (bits >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+
+
+def gaussian(seed: int, stream: int, n: int) -> np.ndarray:
+    """n standard normals by Box-Muller."""
+    m = (n + 1) // 2
+    u1 = uniform53(seed, 2 * stream, m)
+    u2 = uniform53(seed, 2 * stream + 1, m)
+    r = np.sqrt(-2.0 * np.log1p(-u1))
+    z = np.concatenate([r * np.cos(2 * np.pi * u2), r * np.sin(2 * np.pi * u2)])
+    return z[:n]
+
+
+def mirror_extend(octant: np.ndarray) -> np.ndarray:
+    """Full grid from its first octant with f[i] = f[N-1-i] on every axis."""
+    f = np.concatenate([octant, octant[::-1]], axis=0)
+    f = np.concatenate([f, f[:, ::-1]], axis=1)
+    return np.concatenate([f, f[:, :, ::-1]], axis=2)
+
+
+def seed_fields(N, L, phase: str = "BCC", A: float = 2.0, sigma: float = 0.01, seed: int = 20261203):
+    """Full-grid (N0, N1, N2) fields wA, wB (all N even)."""
+    N = tuple(int(v) for v in N)
+    L = tuple(float(v) for v in (L if np.ndim(L) else (L, L, L)))
+    if any(v % 2 for v in N):
+        raise ValueError("grid sizes must be even")
+    oct_shape = tuple(v // 2 for v in N)
+    # evaluated on the first octant and mirrored, so the symmetry holds bit for bit
+    c = [np.cos(2 * np.pi * (np.arange(oct_shape[d]) + 0.5) / N[d]) for d in range(3)]
+    cx, cy, cz = c[0][:, None, None], c[1][None, :, None], c[2][None, None, :]
+    if phase.upper() == "BCC":
+        S = cx * cy + cy * cz + cz * cx
+    elif phase.upper() == "FCC":
+        S = cx * cy * cz
+    else:
+        raise ValueError("phase must be BCC or FCC")
+    S = np.broadcast_to(S, oct_shape)
+    n = int(np.prod(oct_shape))
+    nA = sigma * gaussian(seed, 0, n).reshape(oct_shape)
+    nB = sigma * gaussian(seed, 1, n).reshape(oct_shape)
+    wA = np.ascontiguousarray(mirror_extend(A * S + nA))
+    wB = np.ascontiguousarray(mirror_extend(-A * S + nB))
+    return wA, wB
+
+
+def to_physical(kind: str, full: np.ndarray) -> np.ndarray:
+    """main()'s per-solver field extraction (src/crysSCFT_sample.cpp:202-258)."""
+    kind = kind.upper()
+    if kind == "P1":
+        return np.ascontiguousarray(full)
+    if kind == "3M":
+        return np.ascontiguousarray(full[::2, ::2, ::2])
+    n0, n1, n2 = (v // 2 for v in full.shape)
+    return np.ascontiguousarray(full[:n0, :n1, :n2])
+
+
+def from_physical(kind: str, phy: np.ndarray, N) -> np.ndarray:
+    """Inverse of to_physical for mirror-symmetric fields."""
+    kind = kind.upper()
+    if kind == "P1":
+        return np.asarray(phy).reshape(N)
+    if kind == "PMMM":
+        return mirror_extend(np.asarray(phy).reshape(tuple(v // 2 for v in N)))
+    # 3M: even sub-lattice point 2i; its mirror partner N-1-2i is odd
+    full = np.empty(N)
+    ev = np.asarray(phy).reshape(tuple(v // 2 for v in N))
+    idx = [np.empty(N[d], dtype=np.int64) for d in range(3)]
+    for d in range(3):
+        i = np.arange(N[d] // 2)
+        idx[d][2 * i] = i
+        idx[d][N[d] - 1 - 2 * i] = i
+    full[...] = ev[np.ix_(idx[0], idx[1], idx[2])]
+    return full

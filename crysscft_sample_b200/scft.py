@@ -1,0 +1,152 @@
+"""Python mirror of the reference's SCFT driver (src/crysSCFT_sample.cpp), backed by the
+B200 library.
+
+* ``solve_diffusion_equation`` — src/crysSCFT_sample.cpp:373-396, through
+  ``scft_solver_propagate`` (host buffers) with the same arguments and the same
+  slot convention (direction +1 fills slots 0..Ns, -1 fills Ns..0).
+* ``DiblockSCFT`` — the device-resident AB-diblock iteration (the loop of
+  ``diblock_scft_simple_iterate``, :440-508) behind ``scft_diblock_*``.
+* ``diblock_scft_simple_iterate`` — the driver itself with the reference's
+  arguments and printout (:426-531).
+"""
+from __future__ import annotations
+
+import ctypes
+import time
+
+import numpy as np
+
+from . import _lib
+from ._lib import check
+
+__all__ = ["solve_diffusion_equation", "DiblockSCFT", "diblock_scft_simple_iterate", "contour_counts"]
+
+
+def contour_counts(fA: float, ds: float):
+    """NsA = size_t(fA/ds), NsB = size_t((1-fA)/ds) (src/crysSCFT_sample.cpp:442-444)."""
+    return int(fA / ds), int((1 - fA) / ds)
+
+
+def solve_diffusion_equation(q, init, wds, solver, Ns: int, direction: int):
+    """Fill q[(Ns+1)*M] (numpy float64) with the propagator; returns q."""
+    if direction not in (1, -1):
+        raise _lib.ScftError(1, "Wrong direction")
+    M = solver.get_space_size_phy()
+    q = np.asarray(q)
+    if q.dtype != np.float64 or not q.flags["C_CONTIGUOUS"] or q.size < (Ns + 1) * M:
+        raise ValueError("q must be a contiguous float64 array of (Ns+1)*space_size_phy")
+    init = np.ascontiguousarray(init, dtype=np.float64).ravel()
+    wds = np.ascontiguousarray(wds, dtype=np.float64).ravel()
+    check(_lib.load().scft_solver_propagate(solver.handle, _lib.dptr(q), _lib.dptr(init), _lib.dptr(wds),
+                                            int(Ns), int(direction)))
+    return q
+
+
+class DiblockSCFT:
+    """AB-diblock SCFT with simple mixing, resident on the GPU.
+
+    One ``iterate()`` step is one pass of the reference loop body
+    (src/crysSCFT_sample.cpp:476-508): Boltzmann factors, the four propagator
+    chains, Q, phi (trapezoid), free energy, field update.
+    """
+
+    def __init__(self, solver, fA: float, ds: float, xN: float, acceptance: float):
+        self.solver = solver
+        h = ctypes.c_void_p()
+        check(_lib.load().scft_diblock_create(solver.handle, float(fA), float(ds), float(xN), float(acceptance),
+                                              ctypes.byref(h)))
+        self._h = h
+        self.fA, self.ds, self.xN, self.acceptance = fA, ds, xN, acceptance
+        a, b = ctypes.c_size_t(), ctypes.c_size_t()
+        check(_lib.load().scft_diblock_get_contour_counts(self._h, ctypes.byref(a), ctypes.byref(b)))
+        self.NsA, self.NsB = a.value, b.value
+        self.M = solver.get_space_size_phy()
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().scft_diblock_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_fields(self, wA, wB):
+        wA = np.ascontiguousarray(wA, dtype=np.float64).ravel()
+        wB = np.ascontiguousarray(wB, dtype=np.float64).ravel()
+        if wA.size != self.M or wB.size != self.M:
+            raise ValueError("fields must have space_size_phy elements")
+        check(_lib.load().scft_diblock_set_fields(self._h, _lib.dptr(wA), _lib.dptr(wB)))
+
+    def get_fields(self):
+        out = [np.empty(self.M) for _ in range(4)]
+        check(_lib.load().scft_diblock_get_fields(self._h, *[_lib.dptr(a) for a in out]))
+        return dict(zip(("phiA", "phiB", "wA", "wB"), out))
+
+    def iterate(self, n_iter: int):
+        """Run n_iter iterations; returns per-iteration F, parts (n,4), maxinc, Q."""
+        F, mi, Q = np.empty(n_iter), np.empty(n_iter), np.empty(n_iter)
+        parts = np.empty((n_iter, 4))
+        check(_lib.load().scft_diblock_iterate(self._h, int(n_iter), _lib.dptr(F), _lib.dptr(parts),
+                                               _lib.dptr(mi), _lib.dptr(Q)))
+        return {"F": F, "parts": parts, "maxinc": mi, "Q": Q}
+
+    def iterate_host(self, wA, wB, n_iter: int):
+        """End-to-end form: host fields in (updated in place), phi and history out."""
+        phiA, phiB = np.empty(self.M), np.empty(self.M)
+        F, mi, Q = np.empty(n_iter), np.empty(n_iter), np.empty(n_iter)
+        parts = np.empty((n_iter, 4))
+        check(_lib.load().scft_diblock_iterate_host(self._h, _lib.dptr(wA), _lib.dptr(wB), int(n_iter),
+                                                    _lib.dptr(phiA), _lib.dptr(phiB), _lib.dptr(F),
+                                                    _lib.dptr(parts), _lib.dptr(mi), _lib.dptr(Q)))
+        return {"F": F, "parts": parts, "maxinc": mi, "Q": Q, "phiA": phiA, "phiB": phiB}
+
+    def device_fields(self):
+        """Raw device pointers (int) of phiA, phiB, wA, wB."""
+        ps = [ctypes.c_void_p() for _ in range(4)]
+        check(_lib.load().scft_diblock_device_fields(self._h, *[ctypes.byref(p) for p in ps]))
+        return tuple(p.value for p in ps)
+
+    def launches_per_iteration(self) -> int:
+        v = ctypes.c_size_t()
+        check(_lib.load().scft_diblock_launches_per_iteration(self._h, ctypes.byref(v)))
+        return v.value
+
+
+def diblock_scft_simple_iterate(Nx, Ny, Nz, fA, ds, xN, Lx, Ly, Lz, acceptance, Nstep, solvername, solver,
+                                init_func, verbose: bool = True):
+    """src/crysSCFT_sample.cpp:426-531 on the GPU: init_func(wA, wB) fills numpy arrays of
+    space_size_phy; prints every 10 iterations and the last (:502-503).  Returns the
+    history dict plus the final phi/w fields and the wall time of the loop."""
+    M = solver.get_space_size_phy()
+    wA = np.empty(M)
+    wB = np.empty(M)
+    init_func(wA, wB)
+    solver.set_cell_para((Lx, Ly, Lz))
+    solver.set_contour_step(ds)
+    run = DiblockSCFT(solver, fA, ds, xN, acceptance)
+    run.set_fields(wA, wB)
+    if verbose:
+        print("*" * 66)
+        print(f"Start solving with solver {solvername}...")
+    t0 = time.perf_counter()
+    hist = run.iterate(Nstep)
+    wall = time.perf_counter() - t0
+    if verbose:
+        for itr in range(Nstep):
+            if itr % 10 == 0 or itr == Nstep - 1:
+                eh, e0, e1, ek = hist["parts"][itr]
+                print(f"iter {itr}: FreeEnergy = {hist['F'][itr]:.10g} ( {eh:.10g} + {e0:.10g} + {e1:.10g} + "
+                      f"{ek:.10g} )  , MaxIncompressibility = {hist['maxinc'][itr]:.10g}")
+        print(f"{wall:.6f} s are consumed by {Nstep} iterations")
+        print("*" * 66)
+    hist.update(run.get_fields())
+    hist["wall_seconds"] = wall
+    run.close()
+    return hist

@@ -1,0 +1,148 @@
+/*
+ * crysscft_b200.h — C ABI of the B200 pseudo-spectral propagator library.
+ *
+ * The library replaces the reference's diffusion-solver plugin
+ * (class CrysPSSolverBase, src/solver_base.h:8-51, and its three
+ * implementations CrysPSSolverP1, CrysPSSolver3m, CrysPSSolverPmmm) and the
+ * contour/iteration loop that drives it (src/crysSCFT_sample.cpp:373-531).
+ * Every entry point takes plain pointers and sizes and returns an int status
+ * (SCFT_OK == 0).  Host pointers are ordinary (pageable or pinned) memory;
+ * "_device" entry points take device pointers on the solver's GPU and an
+ * optional cudaStream_t passed as void* (NULL = the solver's own stream).
+ *
+ * Grids are C-ordered (x slowest, z fastest) like the reference.  "Logical"
+ * sizes are the full-cell grid (Nx, Ny, Nz); "physical" sizes are what the
+ * solver stores: the full grid for P1, (Nx/2, Ny/2, Nz/2) for 3M and PMMM.
+ *
+ * Thread safety: one handle must not be used from two host threads at once
+ * (the reference's solvers are not thread-safe either).
+ */
+#ifndef CRYSSCFT_B200_H
+#define CRYSSCFT_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (the reference prints "ERROR" and calls exit(1)) ---- */
+#define SCFT_OK 0
+#define SCFT_ERR_INVALID_ARG 1   /* null handle/pointer, bad kind, bad direction */
+#define SCFT_ERR_BAD_GRID 2      /* grid rejected (src/solver_p1.h:101-108, solver_3m.h:81-92, solver_Pmmm.h:71-82) */
+#define SCFT_ERR_CUDA 3          /* a CUDA runtime call failed; see scft_last_error() */
+#define SCFT_ERR_ALLOC 4         /* device or pinned allocation failed */
+#define SCFT_ERR_NOT_READY 5     /* set_cell_para / set_contour_step / fields not set yet */
+#define SCFT_ERR_NUMERIC 6       /* NaN/Inf or Q <= 0 detected in an iteration */
+#define SCFT_ERR_TIMEOUT 7       /* a bounded device-side wait gave up */
+#define SCFT_ERR_UNSUPPORTED 8   /* valid request this build does not implement */
+#define SCFT_ERR_NO_DEVICE 9     /* no CUDA device / extension unusable */
+
+/* ---- solver kinds: the reference's three CrysPSSolverBase classes ---- */
+#define SCFT_SOLVER_P1 0   /* CrysPSSolverP1     src/solver_p1.h:14-214  */
+#define SCFT_SOLVER_3M 1   /* CrysPSSolver3m     src/solver_3m.h:14-324  */
+#define SCFT_SOLVER_PMMM 2 /* CrysPSSolverPmmm   src/solver_Pmmm.h:13-215 */
+
+/* ---- arithmetic of the triplets ---- */
+#define SCFT_FP64 0 /* plain form: FP64 everywhere (the reference's arithmetic) */
+#define SCFT_FP32 1 /* FP32 triplets; Q, phi, energy and mixing stay FP64 */
+
+typedef struct scft_solver_s* scft_solver_t;
+typedef struct scft_diblock_s* scft_diblock_t;
+
+/* Text of the last error on this host thread (static storage, never NULL). */
+const char* scft_last_error(void);
+/* Short name of a status code. */
+const char* scft_status_string(int status);
+/* Library version string. */
+const char* scft_version(void);
+
+/* ========================================================================
+ * Solver plugin: replaces CrysPSSolverBase and its implementations.
+ * ======================================================================== */
+
+/* Constructor.  Replaces CrysPSSolverP1(grid) (src/solver_p1.h:16-19),
+ * CrysPSSolver3m(grid, translational_part) (src/solver_3m.h:17-20) and
+ * CrysPSSolverPmmm(grid) (src/solver_Pmmm.h:16-19).  translational_part
+ * (9 doubles, may be NULL = zeros) is used by SCFT_SOLVER_3M only; this build
+ * supports the zero translation the reference's main() uses
+ * (src/crysSCFT_sample.cpp:217) and returns SCFT_ERR_UNSUPPORTED otherwise.
+ * device: CUDA ordinal (-1 = current device). */
+int scft_solver_create(int kind, const size_t grid_size_log[3], const double translational_part[9],
+                       int precision, int device, scft_solver_t* out);
+/* Destructor (~CrysPSSolverP1 etc.).  NULL is accepted. */
+int scft_solver_destroy(scft_solver_t solver);
+
+/* CrysPSSolverBase::set_cell_para (src/solver_base.h:16): {Lx,Ly,Lz,alpha,beta,gamma}.
+ * As in the reference, PMMM uses cell_para[0] for all three axes
+ * (src/solver_Pmmm.h:98-104); P1 and 3M use cell_para[0..2]. */
+int scft_solver_set_cell_para(scft_solver_t solver, const double cell_para[6]);
+/* CrysPSSolverBase::set_contour_step (src/solver_base.h:18).  Operators are cached per ds. */
+int scft_solver_set_contour_step(scft_solver_t solver, double ds);
+
+/* Getters of src/solver_base.h:22-27. */
+int scft_solver_get_grid_size_log(scft_solver_t solver, size_t out[3]);
+int scft_solver_get_grid_size_phy(scft_solver_t solver, size_t out[3]);
+int scft_solver_get_space_size_phy(scft_solver_t solver, size_t* out);
+int scft_solver_get_cell_para(scft_solver_t solver, double out[6]);
+int scft_solver_get_ds(scft_solver_t solver, double* out);
+
+/* CrysPSSolverBase::get_iomat_for_diffusion (src/solver_base.h:28): a host buffer of
+ * space_size_phy doubles owned by the solver (pinned), which diffusion() transforms in place. */
+int scft_solver_get_iomat_for_diffusion(scft_solver_t solver, double** out);
+/* CrysPSSolverBase::diffusion (src/solver_base.h:20): one triplet on the host iomat
+ * (copy to the GPU, triplet, copy back; synchronous). */
+int scft_solver_diffusion(scft_solver_t solver);
+/* One triplet in place on a device buffer of space_size_phy elements (FP64). */
+int scft_solver_diffusion_device(scft_solver_t solver, double* d_io, void* stream);
+
+/* solve_diffusion_equation (src/crysSCFT_sample.cpp:373-396) on device buffers:
+ * q has (Ns+1)*space_size_phy doubles; direction +1 fills slots 0..Ns, -1 fills Ns..0;
+ * every step is q <- wds * T(wds * q). */
+int scft_solver_propagate_device(scft_solver_t solver, double* d_q, const double* d_init,
+                                 const double* d_wds, size_t Ns, int direction, void* stream);
+/* The same on host buffers (copies in and out; synchronous). */
+int scft_solver_propagate(scft_solver_t solver, double* q, const double* init, const double* wds,
+                          size_t Ns, int direction);
+
+/* ========================================================================
+ * AB-diblock SCFT iteration: replaces diblock_scft_simple_iterate
+ * (src/crysSCFT_sample.cpp:426-531) and its helpers (:294-424).
+ * ======================================================================== */
+
+/* Parameters as in the reference driver: NsA = size_t(fA/ds), NsB = size_t((1-fA)/ds)
+ * (src/crysSCFT_sample.cpp:442-444); both must be >= 1.  The solver must have its cell
+ * set; create() calls set_contour_step(ds). */
+int scft_diblock_create(scft_solver_t solver, double fA, double ds, double xN, double acceptance,
+                        scft_diblock_t* out);
+int scft_diblock_destroy(scft_diblock_t d);
+int scft_diblock_get_contour_counts(scft_diblock_t d, size_t* NsA, size_t* NsB);
+
+/* Load wA, wB (space_size_phy doubles each, host). */
+int scft_diblock_set_fields(scft_diblock_t d, const double* wA, const double* wB);
+/* Copy phiA, phiB (of the last iteration) and wA, wB (after its update) to host; any may be NULL. */
+int scft_diblock_get_fields(scft_diblock_t d, double* phiA, double* phiB, double* wA, double* wB);
+/* Device pointers of the resident fields (space_size_phy FP64 each); any out may be NULL. */
+int scft_diblock_device_fields(scft_diblock_t d, double** phiA, double** phiB, double** wA,
+                               double** wB);
+
+/* n_iter iterations on device-resident fields.  Per iteration i the host arrays (each may
+ * be NULL) receive F[i], parts[4*i+0..3] = (enthalpic, -ln Q, entropic, xi term) as
+ * print_energy forms them (src/crysSCFT_sample.cpp:404-418), maxinc[i] and Q[i].
+ * Returns SCFT_ERR_NUMERIC if Q <= 0 or a NaN/Inf shows up. */
+int scft_diblock_iterate(scft_diblock_t d, size_t n_iter, double* F, double* parts,
+                         double* maxinc, double* Q);
+
+/* End-to-end form for callers that keep fields in host memory: copies wA/wB in, runs
+ * n_iter iterations, copies phiA/phiB and the updated wA/wB (in place) back out. */
+int scft_diblock_iterate_host(scft_diblock_t d, double* wA, double* wB, size_t n_iter,
+                              double* phiA, double* phiB, double* F, double* parts,
+                              double* maxinc, double* Q);
+
+/* Number of kernel launches the last scft_diblock_iterate issued per iteration. */
+int scft_diblock_launches_per_iteration(scft_diblock_t d, size_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CRYSSCFT_B200_H */
