@@ -1,0 +1,345 @@
+#!/usr/bin/env python
+"""Benchmark: SCFT iterations/s (and triplets/s) of the AB-diblock BCC system on a
+128^3 full grid with the PmmmDCT solver (64^3 physical grid), Ns = 200 (ds = 0.005),
+fA = 0.25, chiN = 20, L = 4.2 Rg, lambda = 0.1.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision fp64|fp32] [--solver PMMM|3M|P1] [--grid 128]
+
+A step is one SCFT iteration (400 triplets + Q, phi, energy, mixing).  N > 1 runs
+independent replicas, one per GPU (a single instance does not shard); value is the
+sum over ranks of K / (max over ranks of the device time).  Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "SCFT iters/s & triplets/s at 128^3 BCC: FP64 vs FP32+polish at |dF/F|<=1e-8"
+WORKLOAD = dict(fA=0.25, xN=20.0, ds=0.005, L=4.2, acc=0.1, phase="BCC")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64")
+    ap.add_argument("--solver", choices=["PMMM", "3M", "P1"], default="PMMM")
+    ap.add_argument("--grid", type=int, default=128)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload_config(args, extra=None):
+    n = args.grid
+    phy = n if args.solver == "P1" else n // 2
+    cfg = {
+        "workload": (f"AB diblock {WORKLOAD['phase']} {n}^3 full grid, {args.solver} solver on {phy}^3, "
+                     f"Ns=200 (ds={WORKLOAD['ds']}), fA={WORKLOAD['fA']}, chiN={WORKLOAD['xN']}, "
+                     f"L={WORKLOAD['L']} Rg, simple mixing lambda={WORKLOAD['acc']}"),
+        "solver": args.solver,
+        "grid_log": [n, n, n],
+        "grid_phy": [phy, phy, phy],
+        "contour_steps": 200,
+        "precision": args.precision,
+        "parallelism": f"replicas x{args.gpus}",
+        "l2": "inputs larger than L2: the stored contour (2 x 201 slices) is re-read each iteration",
+    }
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.proc = None
+        self.dev = device_index
+
+    def start(self):
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100"]
+        bus = self._bus_id()
+        if bus:
+            cmd += ["-i", bus]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def _bus_id(self):
+        try:
+            import torch
+
+            p = torch.cuda.get_device_properties(self.dev)
+            return f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+        except Exception:
+            return None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out = ""
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU: the reference (compiled as oracle/_ref) on the host cores
+# ---------------------------------------------------------------------------
+def reference_iterations(args, n_iter: int, threads: int | None = None):
+    """Seconds per SCFT iteration of the reference solver on this workload."""
+    import numpy as np
+
+    from crysscft_sample_b200 import fields
+    from oracle import ref
+
+    n = args.grid
+    if threads:
+        ref.set_num_threads(threads)
+    cores = ref.max_threads()
+    wA, wB = fields.seed_fields((n, n, n), WORKLOAD["L"], WORKLOAD["phase"])
+    a, b = fields.to_physical(args.solver, wA), fields.to_physical(args.solver, wB)
+    R = ref.RefSolver(args.solver, (n, n, n))
+    L = (WORKLOAD["L"],) * 3
+    out = R.scft_run(WORKLOAD["fA"], WORKLOAD["ds"], WORKLOAD["xN"], L, WORKLOAD["acc"], n_iter, a, b)
+    return out["wall_seconds"] / n_iter, cores, out
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import numpy as np  # noqa: F401
+
+    from oracle import ref
+
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libscft_ref.so was not built"}))
+        return 0
+    # bounded sample: one untimed iteration, then min(K, cap) timed full iterations
+    per_it, cores, _ = reference_iterations(args, 1)
+    cap = max(1, int(120.0 / max(per_it, 1e-6)))
+    k = max(1, min(args.steps, cap))
+    t0 = time.perf_counter()
+    per_it, cores, _ = reference_iterations(args, k)
+    wall = time.perf_counter() - t0
+    value = 1.0 / per_it
+    U = 200
+    line = {
+        "metric": METRIC, "value": value, "unit": "iterations/s", "n_gpus": args.gpus, "steps": k,
+        "warmup": 1, "ms_per_step": per_it * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded BCC fields)",
+        "impl": "reference", "triplets_per_s": value * 2 * U,
+        "config": workload_config(args),
+        "cpu_baseline": {"value": value, "unit": "iterations/s", "cores": cores, "kind": "reference",
+                         "sample": (f"{k} full SCFT iteration(s) of the same workload ({2 * U} triplets each): "
+                                    "the reference's C++ solvers and driver loop compiled with an FFTW-API "
+                                    f"shim (FFTW absent), OpenMP {cores} threads, wall {wall:.1f} s")},
+        "e2e": {"value": value, "unit": "iterations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    from crysscft_sample_b200 import fields, scft, solvers
+
+    n = args.grid
+    N = (n, n, n)
+    L = WORKLOAD["L"]
+    solver = solvers.make_solver(args.solver, N, precision=args.precision, device=local)
+    stream = torch.cuda.Stream()
+    solver.set_stream(stream)
+    solver.set_cell_para((L, L, L))
+    run = scft.DiblockSCFT(solver, WORKLOAD["fA"], WORKLOAD["ds"], WORKLOAD["xN"], WORKLOAD["acc"])
+    wA, wB = fields.seed_fields(N, L, WORKLOAD["phase"], seed=20261203 + rank)
+    a, b = fields.to_physical(args.solver, wA), fields.to_physical(args.solver, wB)
+    run.set_fields(a, b)
+    M = solver.get_space_size_phy()
+    U = run.NsA + run.NsB
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- device-resident timed region ------------------------------------
+    run.iterate(max(args.warmup, 3))
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    ev0.record(stream)
+    hist = run.iterate(args.steps)
+    ev1.record(stream)
+    ev1.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    ms = max_over_ranks(ms)
+    value = world * args.steps / (ms / 1e3)
+    launches = run.launches_per_iteration()
+    if not np.all(np.isfinite(hist["F"])):
+        raise RuntimeError("non-finite free energy in the timed region")
+
+    # ---- phase timer: the triplet kernels' share (roofline) ---------------
+    phases = run.time_phases(10)
+    chain_ms = phases[1]
+    b = 8 if args.precision == "fp64" else 4
+    alg_bytes_step = 2 * 3 * M * b  # both chains: read q(s), read exp(-w ds/2), write q(s+1)
+    step_s = chain_ms / 1e3 / U
+    achieved = alg_bytes_step / step_s / 1e9
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
+    except Exception:
+        peak, peak_src = 6650.0, "fallback"
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            tj = json.load(f)
+        key = f"{args.solver}_{args.precision}_{n}"
+        traffic = tj.get(key, {}).get("bytes_per_step")
+    except Exception:
+        pass
+
+    # ---- end to end through the host-buffer ABI ---------------------------
+    wA_h = torch.empty(M, dtype=torch.float64, pin_memory=True).numpy()
+    wB_h = torch.empty(M, dtype=torch.float64, pin_memory=True).numpy()
+    fA_, fB_ = run.get_fields()["wA"], run.get_fields()["wB"]
+    wA_h[:] = fA_
+    wB_h[:] = fB_
+    k_e2e = max(10, args.steps // 5)
+    run.iterate_host(wA_h, wB_h, 1)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(k_e2e):
+        run.iterate_host(wA_h, wB_h, 1)
+    e1.record(stream)
+    e1.synchronize()
+    barrier()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    e2e_value = world * k_e2e / (e2e_ms / 1e3)
+
+    line = None
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "iterations/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32",
+            "data": "synthetic (seeded BCC fields, no input file)",
+            "triplets_per_s": value * 2 * U,
+            "config": workload_config(args),
+            "gpu_launches": launches * args.steps,
+            "phases_ms_per_iteration": {"total": phases[0], "triplets": phases[1], "q_phi": phases[2],
+                                        "fields_energy": phases[3]},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "triplet step (z, y, x axis passes; both chains)",
+                         "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured"
+                         else "fallback 6650 GB/s"},
+            "e2e": {"value": e2e_value, "unit": "iterations/s", "h2d_bytes_per_step": 2 * M * 8,
+                    "d2h_bytes_per_step": 4 * M * 8 + 8 * 8},
+            "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"],
+                       "samples": clk["samples"]},
+            "F_last": float(hist["F"][-1]),
+        }
+    if dist is not None:
+        dist.barrier()
+    run.close()
+    solver.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            per_it, cores, _ = reference_iterations(args, 2)
+            line["cpu_baseline"] = {
+                "value": 1.0 / per_it, "unit": "iterations/s", "cores": cores, "kind": "reference",
+                "sample": ("2 full SCFT iterations of the same workload: the reference's C++ solvers and "
+                           "driver loop compiled with an FFTW-API shim (FFTW absent), OpenMP threads"),
+            }
+        except Exception as e:  # the CPU baseline is reported, never required
+            line["cpu_baseline"] = {"value": None, "unit": "iterations/s", "cores": 0, "kind": "reference",
+                                    "sample": f"unavailable: {e}"}
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

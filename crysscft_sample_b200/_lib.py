@@ -50,6 +50,8 @@ SIGNATURES = {
     "scft_diblock_iterate": (ctypes.c_int, [_vp, _sz, _dp, _dp, _dp, _dp]),
     "scft_diblock_iterate_host": (ctypes.c_int, [_vp, _dp, _dp, _sz, _dp, _dp, _dp, _dp, _dp, _dp]),
     "scft_diblock_launches_per_iteration": (ctypes.c_int, [_vp, _szp]),
+    "scft_diblock_time_phases": (ctypes.c_int, [_vp, _sz, _dp]),
+    "scft_solver_set_stream": (ctypes.c_int, [_vp, _vp]),
 }
 
 _lib = None

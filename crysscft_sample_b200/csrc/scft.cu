@@ -154,15 +154,16 @@ struct scft_solver_s {
     std::map<double, std::unique_ptr<OpsSet>> ops_cache;  // per ds, cleared by set_cell_para
     OpsSet* ops = nullptr;
     unsigned long long ops_gen = 0;  // bumped whenever `ops` may point elsewhere
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;      // where work is issued
+    cudaStream_t own_stream = nullptr;  // created by the solver
+    bool user_stream = false;
     double* iomat = nullptr;  // pinned host buffer (get_iomat_for_diffusion)
     DevBuf<double> d_io, d_t1, d_t2;
-    DevBuf<float> f_io, f_t1, f_t2, f_pre;
     size_t launches = 0;
 
     ~scft_solver_s() {
         if (iomat) cudaFreeHost(iomat);
-        if (stream) cudaStreamDestroy(stream);
+        if (own_stream) cudaStreamDestroy(own_stream);
     }
 
     int build_ops(double ds_) {
@@ -233,6 +234,7 @@ struct scft_diblock_s {
     cudaGraphExec_t gexec = nullptr;
     size_t launches_per_iter = 0;
     unsigned long long captured_gen = ~0ULL;
+    cudaEvent_t* phase_events = nullptr;  // set by scft_diblock_time_phases (non-graph runs)
 
     ~scft_diblock_s() {
         if (gexec) cudaGraphExecDestroy(gexec);
@@ -247,6 +249,7 @@ struct scft_diblock_s {
         prep_kernel<T><<<blocks, 256, 0, st>>>(wA.p, wB.p, ksi.p, wAds, wBds, q, qc + U * M, xN, ds, MM);
         CK(cudaGetLastError());
         ++launches;
+        if (phase_events) CK(cudaEventRecord(phase_events[1], st));
         const size_t before = solver->launches;
         for (size_t t_ = 0; t_ < U; ++t_) {
             // forward chain: q[t] -> q[t+1] with block A (t < NsA) or B
@@ -262,12 +265,14 @@ struct scft_diblock_s {
             CKR(solver->triplet<T>(2, io, t1, t2, st));
         }
         launches += solver->launches - before;
+        if (phase_events) CK(cudaEventRecord(phase_events[2], st));
         const int rblocks = (int)std::min<long long>(kRedMaxBlocks, (MM + kRedThreads - 1) / kRedThreads);
         q_reduce_kernel<T><<<rblocks, kRedThreads, 0, st>>>(qc, MM, partials.p, state.p);
         CK(cudaGetLastError());
         phi_kernel<T><<<blocks, 256, 0, st>>>(q, qc, phiA.p, phiB.p, state.p, fA, (long long)NsA,
                                               (long long)NsB, MM);
         CK(cudaGetLastError());
+        if (phase_events) CK(cudaEventRecord(phase_events[3], st));
         energy_kernel<<<rblocks, kRedThreads, 0, st>>>(wA.p, wB.p, phiA.p, phiB.p, ksi.p, xN, MM,
                                                        partials.p, state.p, hist.p, hist_cap);
         CK(cudaGetLastError());
@@ -289,7 +294,8 @@ struct scft_diblock_s {
 
     int ensure_graph() {
         if (gexec) return SCFT_OK;
-        cudaStream_t st = solver->stream;
+        // capture on the solver's own (non-blocking) stream; the graph is launched on solver->stream
+        cudaStream_t st = solver->own_stream;
         CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
         int r = enqueue(st);
         cudaGraph_t g = nullptr;
@@ -363,7 +369,8 @@ int scft_solver_create(int kind, const size_t grid_size_log[3], const double tra
         s->grid_phy[i] = kind == SCFT_SOLVER_P1 ? grid_size_log[i] : grid_size_log[i] / 2;
     }
     s->M = s->grid_phy[0] * s->grid_phy[1] * s->grid_phy[2];
-    CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking));
+    s->stream = s->own_stream;
     cudaError_t e = cudaHostAlloc((void**)&s->iomat, s->M * sizeof(double), cudaHostAllocDefault);
     if (e != cudaSuccess) return fail(SCFT_ERR_ALLOC, "cudaHostAlloc iomat");
     std::memset(s->iomat, 0, s->M * sizeof(double));
@@ -680,6 +687,56 @@ int scft_diblock_iterate_host(scft_diblock_t d, double* wA, double* wB, size_t n
 int scft_diblock_launches_per_iteration(scft_diblock_t d, size_t* out) {
     if (!d || !out) return fail(SCFT_ERR_INVALID_ARG, "null argument");
     *out = d->launches_per_iter;
+    return SCFT_OK;
+}
+
+int scft_diblock_time_phases(scft_diblock_t d, size_t n_iter, double out[4]) {
+    if (!d || !out) return fail(SCFT_ERR_INVALID_ARG, "null argument");
+    if (!d->fields_set) return fail(SCFT_ERR_NOT_READY, "set_fields first");
+    CK(cudaSetDevice(d->solver->device));
+    if (!d->solver->ds_set || !d->solver->ops || d->solver->ds != d->ds)
+        CKR(scft_solver_set_contour_step(d->solver, d->ds));
+    cudaStream_t st = d->solver->stream;
+    cudaEvent_t ev[5];
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    double acc[4] = {0, 0, 0, 0};
+    IterState zero{};
+    CK(cudaMemcpyAsync(d->state.p, &zero, sizeof(IterState), cudaMemcpyHostToDevice, st));
+    for (size_t it = 0; it < n_iter; ++it) {
+        d->phase_events = ev;
+        CK(cudaEventRecord(ev[0], st));
+        CKR(d->enqueue(st));
+        CK(cudaEventRecord(ev[4], st));
+        CK(cudaEventSynchronize(ev[4]));
+        float t01, t12, t23, t04;
+        CK(cudaEventElapsedTime(&t01, ev[0], ev[1]));
+        CK(cudaEventElapsedTime(&t12, ev[1], ev[2]));
+        CK(cudaEventElapsedTime(&t23, ev[2], ev[3]));
+        CK(cudaEventElapsedTime(&t04, ev[0], ev[4]));
+        acc[0] += t04;
+        acc[1] += t12;
+        acc[2] += t23;
+        acc[3] += t04 - t12 - t23;
+        (void)t01;
+    }
+    d->phase_events = nullptr;
+    for (auto& e : ev) cudaEventDestroy(e);
+    for (int i = 0; i < 4; ++i) out[i] = n_iter ? acc[i] / (double)n_iter : 0.0;
+    return SCFT_OK;
+}
+
+int scft_solver_set_stream(scft_solver_t s, void* stream) {
+    if (!s) return fail(SCFT_ERR_INVALID_ARG, "null handle");
+    CK(cudaSetDevice(s->device));
+    if (s->user_stream) CK(cudaStreamSynchronize(s->stream));
+    if (!stream) {
+        if (s->user_stream) s->stream = s->own_stream;
+        s->user_stream = false;
+    } else {
+        CK(cudaStreamSynchronize(s->stream));
+        s->stream = (cudaStream_t)stream;
+        s->user_stream = true;
+    }
     return SCFT_OK;
 }
 

@@ -113,6 +113,12 @@ class DiblockSCFT:
         check(_lib.load().scft_diblock_device_fields(self._h, *[ctypes.byref(p) for p in ps]))
         return tuple(p.value for p in ps)
 
+    def time_phases(self, n_iter: int):
+        """ms per iteration: (total, propagator chains, Q + phi, the rest); advances the fields."""
+        out = np.zeros(4)
+        check(_lib.load().scft_diblock_time_phases(self._h, int(n_iter), _lib.dptr(out)))
+        return tuple(out)
+
     def launches_per_iteration(self) -> int:
         v = ctypes.c_size_t()
         check(_lib.load().scft_diblock_launches_per_iteration(self._h, ctypes.byref(v)))

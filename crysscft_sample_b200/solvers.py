@@ -108,6 +108,10 @@ class CrysPSSolverBase:
         return self._iomat
 
     # -- device-resident extras ---------------------------------------------
+    def set_stream(self, stream=None):
+        """Issue work on a torch.cuda.Stream (or raw cudaStream_t); None = the solver's own."""
+        check(_lib.load().scft_solver_set_stream(self._h, _stream_ptr(stream)))
+
     def diffusion_device(self, t, stream=None):
         """One triplet in place on a torch float64 CUDA tensor of space_size_phy elements."""
         _check_tensor(t, self._space_phy)

@@ -142,6 +142,17 @@ int scft_diblock_iterate_host(scft_diblock_t d, double* wA, double* wB, size_t n
 /* Number of kernel launches the last scft_diblock_iterate issued per iteration. */
 int scft_diblock_launches_per_iteration(scft_diblock_t d, size_t* out);
 
+/* Phase timer, the GPU counterpart of the reference's std::clock() sum around
+ * diffusion() (src/crysSCFT_sample.cpp:389-391): runs n_iter iterations without the
+ * CUDA graph, with CUDA events between phases, and returns milliseconds per iteration:
+ * out[0] whole iteration, out[1] the propagator chains (all triplets), out[2] Q + phi,
+ * out[3] Boltzmann factors + energy + field update.  The fields advance as in iterate(). */
+int scft_diblock_time_phases(scft_diblock_t d, size_t n_iter, double out[4]);
+
+/* Make the solver (and every diblock built on it) issue its work on `stream`
+ * (a cudaStream_t; NULL restores the solver's own stream). */
+int scft_solver_set_stream(scft_solver_t solver, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

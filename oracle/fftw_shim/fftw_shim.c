@@ -50,6 +50,8 @@ static cplan* g_cplans = NULL;
 
 static cplan* cplan_get(int n) {
     cplan* p;
+    for (p = __atomic_load_n(&g_cplans, __ATOMIC_ACQUIRE); p; p = p->next)
+        if (p->n == n) return p;
 #ifdef _OPENMP
 #pragma omp critical(crysscft_shim_plan)
 #endif
@@ -74,7 +76,7 @@ static cplan* cplan_get(int n) {
                 p->wim[k] = (double)sinl(a);
             }
             p->next = g_cplans;
-            g_cplans = p;
+            __atomic_store_n(&g_cplans, p, __ATOMIC_RELEASE);
         }
     }
     return p;
@@ -311,6 +313,8 @@ typedef struct hplan {
 static hplan* g_hplans = NULL;
 static hplan* hplan_get(int n) {
     hplan* p;
+    for (p = __atomic_load_n(&g_hplans, __ATOMIC_ACQUIRE); p; p = p->next)
+        if (p->n == n) return p;
 #ifdef _OPENMP
 #pragma omp critical(crysscft_shim_plan)
 #endif
@@ -328,7 +332,7 @@ static hplan* hplan_get(int n) {
                 p->s[k] = (double)sinl(a);
             }
             p->next = g_hplans;
-            g_hplans = p;
+            __atomic_store_n(&g_hplans, p, __ATOMIC_RELEASE);
         }
     }
     return p;
@@ -689,11 +693,19 @@ static void exec_r2r(const fftw_plan p) {
     const int n0 = p->n[0], n1 = p->n[1], n2 = p->n[2];
     const size_t tot = (size_t)n0 * n1 * n2;
     double* R = (double*)malloc(sizeof(double) * tot);
-    memcpy(R, p->in, sizeof(double) * tot);
+    const double* src = (const double*)p->in;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static)
+#endif
+    for (long i = 0; i < (long)tot; ++i) R[i] = src[i];
     r2r_axis(R, (long)n0 * n1, n2, 1, p->kind[2]);
     r2r_axis(R, n0, n1, n2, p->kind[1]);
     r2r_axis(R, 1, n0, (long)n1 * n2, p->kind[0]);
-    memcpy(p->out, R, sizeof(double) * tot);
+    double* dst = (double*)p->out;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static)
+#endif
+    for (long i = 0; i < (long)tot; ++i) dst[i] = R[i];
     free(R);
 }
 
