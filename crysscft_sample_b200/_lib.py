@@ -52,6 +52,7 @@ SIGNATURES = {
     "scft_diblock_launches_per_iteration": (ctypes.c_int, [_vp, _szp]),
     "scft_diblock_time_phases": (ctypes.c_int, [_vp, _sz, _dp]),
     "scft_solver_set_stream": (ctypes.c_int, [_vp, _vp]),
+    "scft_solver_diffusion_device_static_scratch": (ctypes.c_int, [_vp, _vp, _vp]),
 }
 
 _lib = None

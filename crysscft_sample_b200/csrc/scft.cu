@@ -11,6 +11,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -741,3 +742,57 @@ int scft_solver_set_stream(scft_solver_t s, void* stream) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Triplet with library-owned static scratch (allocates nothing per call).
+//
+// For callers that cannot allocate device memory themselves or through us: an
+// application whose device memory is entirely owned by another framework's pool
+// (a fresh cudaMalloc could fail or fragment that pool), or a code path that must
+// not run cudaMalloc/cudaFree because those calls can synchronise the device.
+// The two intermediate fields of the three axis passes live in the file-scope
+// array below instead of solver-owned cudaMalloc'd buffers.  Every GPU that loads
+// this library holds the array (2 x SCFT_STATIC_SCRATCH_MAX_POINTS doubles, 4 MiB)
+// until the process exits.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) double g_static_triplet_scratch[2 * SCFT_STATIC_SCRATCH_MAX_POINTS];
+
+namespace {
+constexpr int kMaxStaticDevices = 64;
+std::mutex g_static_scratch_mu;
+double* g_static_scratch_dev[kMaxStaticDevices] = {};  // device address per ordinal, set once
+}  // namespace
+
+extern "C" int scft_solver_diffusion_device_static_scratch(scft_solver_t s, double* d_io, void* stream) {
+    CKR(solver_ready(s));
+    if (!d_io) return fail(SCFT_ERR_INVALID_ARG, "null buffer");
+    if (s->M > (size_t)SCFT_STATIC_SCRATCH_MAX_POINTS)
+        return fail(SCFT_ERR_INVALID_ARG,
+                    "static-scratch triplet: space_size_phy " + std::to_string(s->M) + " exceeds the maximum " +
+                        std::to_string((size_t)SCFT_STATIC_SCRATCH_MAX_POINTS));
+    if (s->device < 0 || s->device >= kMaxStaticDevices)
+        return fail(SCFT_ERR_INVALID_ARG, "static-scratch triplet: device ordinal out of range");
+    CK(cudaSetDevice(s->device));
+    double* scratch = nullptr;
+    {
+        // one-time set-up per device, with that device current: the host-side name of the
+        // array is not a device address, so ask the runtime for the address on this device
+        std::lock_guard<std::mutex> lock(g_static_scratch_mu);
+        if (!g_static_scratch_dev[s->device]) {
+            void* p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_static_triplet_scratch);
+            if (e != cudaSuccess || !p)
+                return fail(SCFT_ERR_CUDA, std::string("cudaGetSymbolAddress(static scratch): ") +
+                                               cudaGetErrorString(e));
+            g_static_scratch_dev[s->device] = static_cast<double*>(p);
+        }
+        scratch = g_static_scratch_dev[s->device];
+    }
+    cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
+    // the z pass writes every element of t1 before the y pass reads it, and the y pass
+    // writes every element of t2 before the x pass reads it: nothing needs clearing
+    ChainIO<double> io[2] = {{d_io, d_io, nullptr, nullptr}, {}};
+    double* t1[2] = {scratch, nullptr};
+    double* t2[2] = {scratch + SCFT_STATIC_SCRATCH_MAX_POINTS, nullptr};
+    return s->triplet<double>(1, io, t1, t2, st);
+}

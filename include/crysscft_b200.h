@@ -149,6 +149,24 @@ int scft_diblock_launches_per_iteration(scft_diblock_t d, size_t* out);
  * out[3] Boltzmann factors + energy + field update.  The fields advance as in iterate(). */
 int scft_diblock_time_phases(scft_diblock_t d, size_t n_iter, double out[4]);
 
+/* One triplet in place on a device buffer, like scft_solver_diffusion_device, but
+ * allocating nothing: no cudaMalloc, cudaFree or allocating library call, ever.
+ * No counterpart in the reference (its solvers allocate on the host in their
+ * constructors).  It is for callers that cannot allocate device memory: programs
+ * whose device memory is entirely owned by another framework's pool, and code paths
+ * that must not call cudaMalloc/cudaFree because those calls can synchronise the
+ * device.  The solver itself (operators) must have been set up beforehand.
+ * Scratch: a static device array inside the library of
+ * 2 x SCFT_STATIC_SCRATCH_MAX_POINTS doubles (4 MiB), held by every GPU that loads
+ * the library until the process exits.  Solvers with space_size_phy above
+ * SCFT_STATIC_SCRATCH_MAX_POINTS are rejected with SCFT_ERR_INVALID_ARG.  The first
+ * call on each device looks up the array's device address (cudaGetSymbolAddress);
+ * make that first call before any stream capture.  All calls on a device share the
+ * one array, so calls that overlap on the GPU (different streams, or different
+ * host threads) race and corrupt each other's results: serialise them. */
+#define SCFT_STATIC_SCRATCH_MAX_POINTS 262144
+int scft_solver_diffusion_device_static_scratch(scft_solver_t solver, double* d_io, void* stream);
+
 /* Make the solver (and every diblock built on it) issue its work on `stream`
  * (a cudaStream_t; NULL restores the solver's own stream). */
 int scft_solver_set_stream(scft_solver_t solver, void* stream);
