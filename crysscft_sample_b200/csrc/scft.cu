@@ -17,6 +17,7 @@
 
 #include "../../include/crysscft_b200.h"
 #include "axis_kernels.cuh"
+#include "contour_kernel.cuh"
 #include "field_kernels.cuh"
 #include "operators.h"
 
@@ -75,7 +76,50 @@ struct DevBuf {
 struct OpsSet {
     DevBuf<double> d_op[3], d_opT[3];
     DevBuf<float> f_op[3], f_opT[3];
+    // packed per-axis operators for the persistent contour kernel (FP64): for an
+    // even/odd axis E then O (h x h, leading dimension h+4), else A (n x n, n+4)
+    std::vector<double> h_packed;
+    DevBuf<double> d_packed;
+    int eo[3] = {0, 0, 0}, off[3] = {0, 0, 0}, ld[3] = {0, 0, 0}, half[3] = {0, 0, 0};
+    int total = 0;
 };
+
+// Append one axis operator to the packed buffer, in even/odd form when A is
+// centrosymmetric (A[n-1-i][n-1-j] == A[i][j]) and n is a multiple of 16.
+void pack_operator(const std::vector<long double>& A, int n, OpsSet& s, int axis) {
+    bool centro = (n % 16 == 0);
+    for (int i = 0; centro && i < n; ++i)
+        for (int j = 0; j < n; ++j) {
+            const long double a = A[(size_t)i * n + j], b = A[(size_t)(n - 1 - i) * n + (n - 1 - j)];
+            if (fabsl(a - b) > 1e-17L * (1.0L + fabsl(a))) { centro = false; break; }
+        }
+    s.off[axis] = (int)s.h_packed.size();
+    if (centro) {
+        const int h = n / 2, ld = h + 4;
+        s.eo[axis] = 1;
+        s.ld[axis] = ld;
+        s.half[axis] = h * ld;
+        s.h_packed.resize(s.h_packed.size() + 2 * (size_t)h * ld, 0.0);
+        double* E = s.h_packed.data() + s.off[axis];
+        double* O = E + (size_t)h * ld;
+        for (int i = 0; i < h; ++i)
+            for (int j = 0; j < h; ++j) {
+                const long double a = A[(size_t)i * n + j], b = A[(size_t)i * n + (n - 1 - j)];
+                E[(size_t)i * ld + j] = (double)((a + b) / 2);
+                O[(size_t)i * ld + j] = (double)((a - b) / 2);
+            }
+    } else {
+        const int ld = n + 4;
+        s.eo[axis] = 0;
+        s.ld[axis] = ld;
+        s.half[axis] = 0;
+        s.h_packed.resize(s.h_packed.size() + (size_t)n * ld, 0.0);
+        double* D = s.h_packed.data() + s.off[axis];
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) D[(size_t)i * ld + j] = (double)A[(size_t)i * n + j];
+    }
+    s.total = (int)s.h_packed.size();
+}
 
 int upload_operator(const std::vector<long double>& A, int n, OpsSet& s, int axis) {
     std::vector<double> d((size_t)n * n), dt((size_t)n * n);
@@ -179,7 +223,11 @@ struct scft_solver_s {
             else
                 A = m3_axis_operator(N, (long double)cell[ax], (long double)ds_);
             CKR(upload_operator(A, (int)grid_phy[ax], *s, ax));
+            pack_operator(A, (int)grid_phy[ax], *s, ax);
         }
+        CKR(s->d_packed.alloc(s->h_packed.size()));
+        CK(cudaMemcpy(s->d_packed.p, s->h_packed.data(), s->h_packed.size() * sizeof(double),
+                      cudaMemcpyHostToDevice));
         ops = s.get();
         ops_cache[ds_] = std::move(s);
         ++ops_gen;
@@ -236,10 +284,91 @@ struct scft_diblock_s {
     size_t launches_per_iter = 0;
     unsigned long long captured_gen = ~0ULL;
     cudaEvent_t* phase_events = nullptr;  // set by scft_diblock_time_phases (non-graph runs)
+    bool use_graph = true;                // cleared if a capture is refused
+    bool persistent = false;              // whole-contour cooperative kernel eligible
+    int persistent_grid = 0;
+    size_t persistent_smem = 0;
+    DevBuf<unsigned> ctrl;                // [0] barrier arrivals, [1] error bits
+    long long spin_limit = 20000000LL;
 
     ~scft_diblock_s() {
         if (gexec) cudaGraphExecDestroy(gexec);
         if (graph) cudaGraphDestroy(graph);
+    }
+
+    // Decide whether the persistent contour kernel can run this grid (FP64, every
+    // axis a multiple of 8 and at most kContourMaxN, shared memory within the limit).
+    int setup_persistent() {
+        persistent = false;
+        if (precision != SCFT_FP64) return SCFT_OK;
+        const OpsSet* o = solver->ops;
+        if (!o) return SCFT_OK;
+        for (int ax = 0; ax < 3; ++ax) {
+            const size_t n = solver->grid_phy[ax];
+            if (n < 8 || n % 8 || n > (size_t)kContourMaxN) return SCFT_OK;
+        }
+        const int nx = (int)solver->grid_phy[0], ny = (int)solver->grid_phy[1], nz = (int)solver->grid_phy[2];
+        const int rows = nx > ny ? nx : ny;
+        const size_t smem = ((size_t)((o->total + 1) & ~1) + 2 * (size_t)rows * (nz + 4)) * sizeof(double);
+        int dev_smem = 0, sms = 0;
+        CK(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, solver->device));
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, solver->device));
+        if (smem > (size_t)dev_smem) return SCFT_OK;
+        CK(cudaFuncSetAttribute(contour_kernel_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int per_sm = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, contour_kernel_f64, kContourThreads, smem));
+        if (per_sm < 1) return SCFT_OK;
+        const int units = 2 * (nx > ny ? nx : ny);
+        persistent_grid = std::min(units, per_sm * sms);
+        persistent_smem = smem;
+        if (!ctrl.p) CKR(ctrl.alloc(2));
+        CK(cudaMemset(ctrl.p, 0, 2 * sizeof(unsigned)));
+        persistent = true;
+        return SCFT_OK;
+    }
+
+    int launch_contour(cudaStream_t st, double* wAds, double* wBds, double* q, double* qc) {
+        const OpsSet* o = solver->ops;
+        ContourArgs a{};
+        a.q[0] = q;
+        a.q[1] = qc;
+        a.wds[0] = wAds;
+        a.wds[1] = wBds;
+        a.xbuf[0] = d_t[0].p;
+        a.xbuf[1] = d_t[1].p;
+        a.ops = o->d_packed.p;
+        for (int ax = 0; ax < 3; ++ax) {
+            a.n[ax] = (int)solver->grid_phy[ax];
+            a.eo[ax] = o->eo[ax];
+            a.op_off[ax] = o->off[ax];
+            a.op_ld[ax] = o->ld[ax];
+            a.op_half[ax] = o->half[ax];
+        }
+        a.ops_total = o->total;
+        a.nchain = 2;
+        a.slot0[0] = 0;
+        a.dir[0] = 1;
+        a.slot0[1] = (long long)U;
+        a.dir[1] = -1;
+        a.NsA = (long long)NsA;
+        a.t_begin = 0;
+        a.t_end = (int)U;
+        a.bar_count = ctrl.p;
+        a.error = reinterpret_cast<int*>(ctrl.p + 1);
+        a.spin_limit = spin_limit;
+        CK(cudaMemsetAsync(ctrl.p, 0, sizeof(unsigned), st));
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3((unsigned)persistent_grid);
+        cfg.blockDim = dim3(kContourThreads);
+        cfg.dynamicSmemBytes = persistent_smem;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        CK(cudaLaunchKernelEx(&cfg, contour_kernel_f64, a));
+        return SCFT_OK;
     }
 
     template <typename T>
@@ -252,7 +381,13 @@ struct scft_diblock_s {
         ++launches;
         if (phase_events) CK(cudaEventRecord(phase_events[1], st));
         const size_t before = solver->launches;
-        for (size_t t_ = 0; t_ < U; ++t_) {
+        if constexpr (sizeof(T) == 8) {
+            if (persistent) {
+                CKR(launch_contour(st, wAds, wBds, q, qc));
+                ++solver->launches;
+            }
+        }
+        for (size_t t_ = 0; t_ < U && !(persistent && sizeof(T) == 8); ++t_) {
             // forward chain: q[t] -> q[t+1] with block A (t < NsA) or B
             // backward chain: qc[U-t] -> qc[U-t-1] with the block of segment U-t-1
             const T* w1 = t_ < NsA ? wAds : wBds;
@@ -294,21 +429,37 @@ struct scft_diblock_s {
     }
 
     int ensure_graph() {
-        if (gexec) return SCFT_OK;
+        if (gexec || !use_graph) return SCFT_OK;
         // capture on the solver's own (non-blocking) stream; the graph is launched on solver->stream
         cudaStream_t st = solver->own_stream;
         CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
         int r = enqueue(st);
         cudaGraph_t g = nullptr;
         cudaError_t e = cudaStreamEndCapture(st, &g);
-        if (r != SCFT_OK) {
+        if (r != SCFT_OK || e != cudaSuccess) {
+            // capture refused (e.g. a launch form the runtime cannot record): run uncaptured
             if (g) cudaGraphDestroy(g);
-            return r;
+            cudaGetLastError();
+            use_graph = false;
+            return SCFT_OK;
         }
-        if (e != cudaSuccess) return fail(SCFT_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
         graph = g;
-        CK(cudaGraphInstantiate(&gexec, graph, 0));
+        if (cudaGraphInstantiate(&gexec, graph, 0) != cudaSuccess) {
+            cudaGetLastError();
+            cudaGraphDestroy(graph);
+            graph = nullptr;
+            gexec = nullptr;
+            use_graph = false;
+        }
         return SCFT_OK;
+    }
+
+    int run_once(cudaStream_t st) {
+        if (gexec) {
+            CK(cudaGraphLaunch(gexec, st));
+            return SCFT_OK;
+        }
+        return enqueue(st);
     }
 };
 
@@ -625,29 +776,51 @@ int scft_diblock_device_fields(scft_diblock_t d, double** phiA, double** phiB, d
     return SCFT_OK;
 }
 
+// Make the operators current and (re)build the launch plan when they changed.
+static int diblock_prepare(scft_diblock_t d, bool want_graph) {
+    if (!d->solver->ds_set || !d->solver->ops || d->solver->ds != d->ds)
+        CKR(scft_solver_set_contour_step(d->solver, d->ds));
+    if (d->captured_gen != d->solver->ops_gen) {
+        if (d->gexec) cudaGraphExecDestroy(d->gexec);
+        if (d->graph) cudaGraphDestroy(d->graph);
+        d->gexec = nullptr;
+        d->graph = nullptr;
+        CKR(d->setup_persistent());
+        d->captured_gen = d->solver->ops_gen;
+    }
+    if (want_graph) CKR(d->ensure_graph());
+    return SCFT_OK;
+}
+
+// Read and clear the device-side error bits of the persistent kernel.
+static int diblock_check_device_error(scft_diblock_t d, cudaStream_t st) {
+    if (!d->ctrl.p) return SCFT_OK;
+    unsigned e = 0;
+    CK(cudaMemcpyAsync(&e, d->ctrl.p + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (e) {
+        CK(cudaMemsetAsync(d->ctrl.p + 1, 0, sizeof(unsigned), st));
+        CK(cudaStreamSynchronize(st));
+        return fail(SCFT_ERR_TIMEOUT, "a grid barrier of the contour kernel gave up waiting");
+    }
+    return SCFT_OK;
+}
+
 static int diblock_run(scft_diblock_t d, size_t n_iter, double* F, double* parts, double* maxinc,
                        double* Q) {
     cudaStream_t st = d->solver->stream;
-    if (!d->solver->ds_set || !d->solver->ops || d->solver->ds != d->ds)
-        CKR(scft_solver_set_contour_step(d->solver, d->ds));
-    if (d->gexec && d->captured_gen != d->solver->ops_gen) {
-        cudaGraphExecDestroy(d->gexec);
-        cudaGraphDestroy(d->graph);
-        d->gexec = nullptr;
-        d->graph = nullptr;
-    }
-    CKR(d->ensure_graph());
-    d->captured_gen = d->solver->ops_gen;
+    CKR(diblock_prepare(d, true));
     size_t done = 0;
     std::vector<double> h;
     while (done < n_iter) {
         const size_t chunk = std::min<size_t>(n_iter - done, d->hist_cap);
         IterState zero{};
         CK(cudaMemcpyAsync(d->state.p, &zero, sizeof(IterState), cudaMemcpyHostToDevice, st));
-        for (size_t i = 0; i < chunk; ++i) CK(cudaGraphLaunch(d->gexec, st));
+        for (size_t i = 0; i < chunk; ++i) CKR(d->run_once(st));
         h.resize(chunk * HIST_STRIDE);
         CK(cudaMemcpyAsync(h.data(), d->hist.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
+        CKR(diblock_check_device_error(d, st));
         bool bad = false;
         for (size_t i = 0; i < chunk; ++i) {
             const double* r = &h[i * HIST_STRIDE];
@@ -695,8 +868,7 @@ int scft_diblock_time_phases(scft_diblock_t d, size_t n_iter, double out[4]) {
     if (!d || !out) return fail(SCFT_ERR_INVALID_ARG, "null argument");
     if (!d->fields_set) return fail(SCFT_ERR_NOT_READY, "set_fields first");
     CK(cudaSetDevice(d->solver->device));
-    if (!d->solver->ds_set || !d->solver->ops || d->solver->ds != d->ds)
-        CKR(scft_solver_set_contour_step(d->solver, d->ds));
+    CKR(diblock_prepare(d, false));
     cudaStream_t st = d->solver->stream;
     cudaEvent_t ev[5];
     for (auto& e : ev) CK(cudaEventCreate(&e));
@@ -723,7 +895,7 @@ int scft_diblock_time_phases(scft_diblock_t d, size_t n_iter, double out[4]) {
     d->phase_events = nullptr;
     for (auto& e : ev) cudaEventDestroy(e);
     for (int i = 0; i < 4; ++i) out[i] = n_iter ? acc[i] / (double)n_iter : 0.0;
-    return SCFT_OK;
+    return diblock_check_device_error(d, st);
 }
 
 int scft_solver_set_stream(scft_solver_t s, void* stream) {

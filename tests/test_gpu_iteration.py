@@ -33,6 +33,31 @@ def _run_pair(kind, cfg, nstep, precision="fp64"):
 @pytest.mark.parametrize("kind", ["PMMM", "3M", "P1"])
 def test_iterations_match_reference(gpu, kind):
     want, got = _run_pair(kind, CFG0, 20)
+    _compare(want, got)
+
+
+# grids that exercise every launch form: persistent kernel with even/odd axes (64^3 PMMM,
+# 64^3 P1), full-matrix axes (3M), mixed axes (48 = not a multiple of 16), and the
+# per-axis fallback kernels (36 -> 18 is not a multiple of 8; 128 is above the
+# persistent kernel's plane limit)
+SIZES = [
+    ("PMMM", (128, 128, 128), 2),
+    ("3M", (128, 128, 128), 2),
+    ("P1", (64, 64, 64), 2),
+    ("PMMM", (96, 64, 32), 3),
+    ("3M", (36, 32, 48), 3),
+    ("P1", (128, 32, 16), 2),
+]
+
+
+@pytest.mark.parametrize("kind,N,nstep", SIZES)
+def test_iterations_match_reference_sizes(gpu, kind, N, nstep):
+    cfg = dict(CFG0, N=N, ds=0.005)
+    want, got = _run_pair(kind, cfg, nstep)
+    _compare(want, got)
+
+
+def _compare(want, got):
     assert np.all(np.abs(got["F"] - want["F"]) <= F_RTOL * np.abs(want["F"]))
     assert np.abs(got["maxinc"] - want["maxinc"]).max() < 1e-11
     assert np.abs(got["Q"] - want["Q"]).max() < 1e-12 * np.abs(want["Q"]).max()
