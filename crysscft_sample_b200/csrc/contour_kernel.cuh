@@ -345,3 +345,264 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_kernel_f64(const C
 }
 
 }  // namespace crysscft
+
+// ---------------------------------------------------------------------------
+// Compile-time specialised form of the same kernel for common grids: every size,
+// stride and operator offset is a constant, so the tile loops unroll completely.
+// ---------------------------------------------------------------------------
+namespace crysscft {
+
+template <int N, bool EO>
+struct AxisShape {
+    static constexpr int K = EO ? N / 2 : N;       // contraction length
+    static constexpr int LD = K + 4;               // operator leading dimension
+    static constexpr int HALF = EO ? K * LD : 0;   // E -> O offset
+    static constexpr int SIZE = EO ? 2 * K * LD : N * LD;
+};
+
+// G[r][i] = sum_j F[r][j] A[i][j] on an R x C slab (leading dimension LF)
+template <int R, int C, int LF, bool EO>
+__device__ __forceinline__ void row_op_ct(const double* __restrict__ F, double* __restrict__ G,
+                                          const double* __restrict__ opE) {
+    using S = AxisShape<C, EO>;
+    const double* opO = opE + S::HALF;
+    constexpr int NI = S::K, K = S::K;
+    constexpr int TM = R / 8, TN = NI / 8;
+    constexpr int BM = (TM + 1) / 2, BN = (TN + 1) / 2;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll 1
+    for (int blk = warp; blk < BM * BN; blk += kContourThreads / 32) {
+        const int mb = (blk / BN) * 2, nb = (blk % BN) * 2;
+        const bool m1 = (TM % 2 == 0) || (mb + 1 < TM);
+        const bool n1 = (TN % 2 == 0) || (nb + 1 < TN);
+        double dP[2][2][2] = {}, dR[2][2][2] = {};
+        const double* Fr0 = F + (mb * 8 + g) * LF + t;
+        const double* Fr1 = Fr0 + 8 * LF;
+        const double* E0 = opE + (nb * 8 + g) * S::LD + t;
+        const double* E1 = E0 + 8 * S::LD;
+        const double* O0 = opO + (nb * 8 + g) * S::LD + t;
+        const double* O1 = O0 + 8 * S::LD;
+#pragma unroll
+        for (int k0 = 0; k0 < K; k0 += 4) {
+            double aU[2], aV[2];
+            {
+                const double x0 = Fr0[k0];
+                const double x1 = EO ? Fr0[C - 1 - 2 * t - k0] : 0.0;
+                aU[0] = EO ? x0 + x1 : x0;
+                aV[0] = x0 - x1;
+            }
+            if (m1) {
+                const double x0 = Fr1[k0];
+                const double x1 = EO ? Fr1[C - 1 - 2 * t - k0] : 0.0;
+                aU[1] = EO ? x0 + x1 : x0;
+                aV[1] = x0 - x1;
+            } else {
+                aU[1] = aV[1] = 0.0;
+            }
+            const double bE0 = E0[k0];
+            const double bE1 = n1 ? E1[k0] : 0.0;
+            dmma884(dP[0][0], aU[0], bE0);
+            if (n1) dmma884(dP[0][1], aU[0], bE1);
+            if (m1) dmma884(dP[1][0], aU[1], bE0);
+            if (m1 && n1) dmma884(dP[1][1], aU[1], bE1);
+            if (EO) {
+                const double bO0 = O0[k0];
+                const double bO1 = n1 ? O1[k0] : 0.0;
+                dmma884(dR[0][0], aV[0], bO0);
+                if (n1) dmma884(dR[0][1], aV[0], bO1);
+                if (m1) dmma884(dR[1][0], aV[1], bO0);
+                if (m1 && n1) dmma884(dR[1][1], aV[1], bO1);
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+            for (int b = 0; b < 2; ++b) {
+                if ((a == 1 && !m1) || (b == 1 && !n1)) continue;
+                const int r = (mb + a) * 8 + g;
+                const int i = (nb + b) * 8 + 2 * t;
+                if (EO) {
+                    *reinterpret_cast<double2*>(G + r * LF + i) =
+                        make_double2(dP[a][b][0] + dR[a][b][0], dP[a][b][1] + dR[a][b][1]);
+                    *reinterpret_cast<double2*>(G + r * LF + (C - 2 - i)) =
+                        make_double2(dP[a][b][1] - dR[a][b][1], dP[a][b][0] - dR[a][b][0]);
+                } else {
+                    *reinterpret_cast<double2*>(G + r * LF + i) = make_double2(dP[a][b][0], dP[a][b][1]);
+                }
+            }
+    }
+}
+
+// G[i][c] = sum_j A[i][j] F[j][c] on an R x C slab (leading dimension LF)
+template <int R, int C, int LF, bool EO>
+__device__ __forceinline__ void col_op_ct(const double* __restrict__ F, double* __restrict__ G,
+                                          const double* __restrict__ opE) {
+    using S = AxisShape<R, EO>;
+    const double* opO = opE + S::HALF;
+    constexpr int MI = S::K, K = S::K;
+    constexpr int TM = MI / 8, TN = C / 8;
+    constexpr int BM = (TM + 1) / 2, BN = (TN + 1) / 2;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll 1
+    for (int blk = warp; blk < BM * BN; blk += kContourThreads / 32) {
+        const int mb = (blk / BN) * 2, nb = (blk % BN) * 2;
+        const bool m1 = (TM % 2 == 0) || (mb + 1 < TM);
+        const bool n1 = (TN % 2 == 0) || (nb + 1 < TN);
+        double dP[2][2][2] = {}, dR[2][2][2] = {};
+        const double* E0 = opE + (mb * 8 + g) * S::LD + t;
+        const double* E1 = E0 + 8 * S::LD;
+        const double* O0 = opO + (mb * 8 + g) * S::LD + t;
+        const double* O1 = O0 + 8 * S::LD;
+        const double* Fc0 = F + t * LF + nb * 8 + g;         // F[j][c], j = k0 + t
+        const double* Fm0 = F + (R - 1 - t) * LF + nb * 8 + g;  // F[R-1-j][c]
+#pragma unroll
+        for (int k0 = 0; k0 < K; k0 += 4) {
+            double bU[2], bV[2];
+            {
+                const double x0 = Fc0[k0 * LF];
+                const double x1 = EO ? Fm0[-k0 * LF] : 0.0;
+                bU[0] = EO ? x0 + x1 : x0;
+                bV[0] = x0 - x1;
+            }
+            if (n1) {
+                const double x0 = Fc0[k0 * LF + 8];
+                const double x1 = EO ? Fm0[-k0 * LF + 8] : 0.0;
+                bU[1] = EO ? x0 + x1 : x0;
+                bV[1] = x0 - x1;
+            } else {
+                bU[1] = bV[1] = 0.0;
+            }
+            const double aE0 = E0[k0];
+            const double aE1 = m1 ? E1[k0] : 0.0;
+            dmma884(dP[0][0], aE0, bU[0]);
+            if (n1) dmma884(dP[0][1], aE0, bU[1]);
+            if (m1) dmma884(dP[1][0], aE1, bU[0]);
+            if (m1 && n1) dmma884(dP[1][1], aE1, bU[1]);
+            if (EO) {
+                const double aO0 = O0[k0];
+                const double aO1 = m1 ? O1[k0] : 0.0;
+                dmma884(dR[0][0], aO0, bV[0]);
+                if (n1) dmma884(dR[0][1], aO0, bV[1]);
+                if (m1) dmma884(dR[1][0], aO1, bV[0]);
+                if (m1 && n1) dmma884(dR[1][1], aO1, bV[1]);
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+            for (int b = 0; b < 2; ++b) {
+                if ((a == 1 && !m1) || (b == 1 && !n1)) continue;
+                const int i = (mb + a) * 8 + g;
+                const int c = (nb + b) * 8 + 2 * t;
+                if (EO) {
+                    *reinterpret_cast<double2*>(G + i * LF + c) =
+                        make_double2(dP[a][b][0] + dR[a][b][0], dP[a][b][1] + dR[a][b][1]);
+                    *reinterpret_cast<double2*>(G + (R - 1 - i) * LF + c) =
+                        make_double2(dP[a][b][0] - dR[a][b][0], dP[a][b][1] - dR[a][b][1]);
+                } else {
+                    *reinterpret_cast<double2*>(G + i * LF + c) = make_double2(dP[a][b][0], dP[a][b][1]);
+                }
+            }
+    }
+}
+
+// R x C slab between global (row stride gs) and shared memory (row stride LF), optional factor w
+template <bool TO_SMEM, int R, int C, int LF>
+__device__ __forceinline__ void move_slab_ct(double* sm, double* gm, long long gs, const double* w) {
+    constexpr int PER_ROW = C / 2;
+    constexpr int TOTAL = R * PER_ROW;
+    constexpr int U = (TOTAL + kContourThreads - 1) / kContourThreads;
+    double2 v[U], f[U];
+#pragma unroll
+    for (int k = 0; k < U; ++k) {
+        const int e = k * kContourThreads + threadIdx.x;
+        if (TOTAL % kContourThreads == 0 || e < TOTAL) {
+            const int r = e / PER_ROW, c = (e % PER_ROW) * 2;
+            if (TO_SMEM) v[k] = *reinterpret_cast<const double2*>(gm + r * gs + c);
+            else v[k] = *reinterpret_cast<const double2*>(sm + r * LF + c);
+            if (w) f[k] = __ldg(reinterpret_cast<const double2*>(w + r * gs + c));
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < U; ++k) {
+        const int e = k * kContourThreads + threadIdx.x;
+        if (TOTAL % kContourThreads == 0 || e < TOTAL) {
+            const int r = e / PER_ROW, c = (e % PER_ROW) * 2;
+            double2 x = v[k];
+            if (w) {
+                x.x = x.x * f[k].x;
+                x.y = x.y * f[k].y;
+            }
+            if (TO_SMEM) *reinterpret_cast<double2*>(sm + r * LF + c) = x;
+            else *reinterpret_cast<double2*>(gm + r * gs + c) = x;
+        }
+    }
+}
+
+template <int NX, int NY, int NZ, bool EX, bool EY, bool EZ>
+__global__ void __launch_bounds__(kContourThreads, 1) contour_kernel_ct(const ContourArgs a) {
+    extern __shared__ __align__(16) double smem[];
+    constexpr int LF = NZ + 4;
+    constexpr int ROWS = NX > NY ? NX : NY;
+    constexpr int OFFX = 0;
+    constexpr int OFFY = AxisShape<NX, EX>::SIZE;
+    constexpr int OFFZ = OFFY + AxisShape<NY, EY>::SIZE;
+    constexpr int OPS = OFFZ + AxisShape<NZ, EZ>::SIZE;
+    constexpr int OPS_PAD = (OPS + 1) & ~1;
+    double* sops = smem;
+    double* F = smem + OPS_PAD;
+    double* G = F + ROWS * LF;
+    for (int i = threadIdx.x; i < OPS; i += kContourThreads) sops[i] = a.ops[i];
+    __syncthreads();
+
+    constexpr long long M = (long long)NX * NY * NZ;
+    constexpr long long PLANE = (long long)NY * NZ;
+    const int unitsP = a.nchain * NX, unitsQ = a.nchain * NY;
+    unsigned target = 0;
+    for (int t = a.t_begin; t < a.t_end; ++t) {
+        for (int u = blockIdx.x; u < unitsP; u += gridDim.x) {
+            const int c = u >= NX ? 1 : 0, x = u - c * NX;
+            const int dir = c ? a.dir[1] : a.dir[0];
+            const long long in_slot = (c ? a.slot0[1] : a.slot0[0]) + (long long)dir * t;
+            const long long seg = dir > 0 ? in_slot : in_slot - 1;
+            const double* w = seg < a.NsA ? a.wds[0] : a.wds[1];
+            double* q = c ? a.q[1] : a.q[0];
+            double* xb = c ? a.xbuf[1] : a.xbuf[0];
+            move_slab_ct<true, NY, NZ, LF>(F, q + in_slot * M + x * PLANE, NZ, w ? w + x * PLANE : nullptr);
+            __syncthreads();
+            row_op_ct<NY, NZ, LF, EZ>(F, G, sops + OFFZ);
+            __syncthreads();
+            col_op_ct<NY, NZ, LF, EY>(G, F, sops + OFFY);
+            __syncthreads();
+            move_slab_ct<false, NY, NZ, LF>(F, xb + x * PLANE, NZ, nullptr);
+            __syncthreads();
+        }
+        target += gridDim.x;
+        if (!grid_barrier(a.bar_count, a.error, target, a.spin_limit)) return;
+        for (int u = blockIdx.x; u < unitsQ; u += gridDim.x) {
+            const int c = u >= NY ? 1 : 0, y = u - c * NY;
+            const int dir = c ? a.dir[1] : a.dir[0];
+            const long long in_slot = (c ? a.slot0[1] : a.slot0[0]) + (long long)dir * t;
+            const long long out_slot = in_slot + dir;
+            const long long seg = dir > 0 ? in_slot : in_slot - 1;
+            const double* w = seg < a.NsA ? a.wds[0] : a.wds[1];
+            double* q = c ? a.q[1] : a.q[0];
+            double* xb = c ? a.xbuf[1] : a.xbuf[0];
+            move_slab_ct<true, NX, NZ, LF>(F, xb + (long long)y * NZ, PLANE, nullptr);
+            __syncthreads();
+            col_op_ct<NX, NZ, LF, EX>(F, G, sops + OFFX);
+            __syncthreads();
+            move_slab_ct<false, NX, NZ, LF>(G, q + out_slot * M + (long long)y * NZ, PLANE,
+                                            w ? w + (long long)y * NZ : nullptr);
+            __syncthreads();
+        }
+        if (t + 1 < a.t_end) {
+            target += gridDim.x;
+            if (!grid_barrier(a.bar_count, a.error, target, a.spin_limit)) return;
+        }
+    }
+}
+
+}  // namespace crysscft

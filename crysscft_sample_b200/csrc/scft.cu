@@ -181,6 +181,37 @@ cudaError_t launch_axis(const AxisPass<T>& p, int nchain, bool contiguous, cudaS
     return launch_strided_bm<T, 64>(p, nchain, st);
 }
 
+using ContourFn = void (*)(const ContourArgs);
+
+// The compile-time specialised contour kernel for cubic grids (all axes even/odd, or
+// all full), else the runtime-generic one.
+ContourFn contour_kernel_for(int nx, int ny, int nz, const int eo[3]) {
+    if (nx == ny && ny == nz && eo[0] == eo[1] && eo[1] == eo[2]) {
+        if (eo[0]) {
+            switch (nx) {
+                case 16: return contour_kernel_ct<16, 16, 16, true, true, true>;
+                case 32: return contour_kernel_ct<32, 32, 32, true, true, true>;
+                case 48: return contour_kernel_ct<48, 48, 48, true, true, true>;
+                case 64: return contour_kernel_ct<64, 64, 64, true, true, true>;
+                default: break;
+            }
+        } else {
+            switch (nx) {
+                case 8: return contour_kernel_ct<8, 8, 8, false, false, false>;
+                case 16: return contour_kernel_ct<16, 16, 16, false, false, false>;
+                case 24: return contour_kernel_ct<24, 24, 24, false, false, false>;
+                case 32: return contour_kernel_ct<32, 32, 32, false, false, false>;
+                case 40: return contour_kernel_ct<40, 40, 40, false, false, false>;
+                case 48: return contour_kernel_ct<48, 48, 48, false, false, false>;
+                case 56: return contour_kernel_ct<56, 56, 56, false, false, false>;
+                case 64: return contour_kernel_ct<64, 64, 64, false, false, false>;
+                default: break;
+            }
+        }
+    }
+    return contour_kernel_f64;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -288,6 +319,7 @@ struct scft_diblock_s {
     bool persistent = false;              // whole-contour cooperative kernel eligible
     int persistent_grid = 0;
     size_t persistent_smem = 0;
+    ContourFn contour_fn = nullptr;
     DevBuf<unsigned> ctrl;                // [0] barrier arrivals, [1] error bits
     long long spin_limit = 20000000LL;
 
@@ -314,9 +346,10 @@ struct scft_diblock_s {
         CK(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, solver->device));
         CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, solver->device));
         if (smem > (size_t)dev_smem) return SCFT_OK;
-        CK(cudaFuncSetAttribute(contour_kernel_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        contour_fn = contour_kernel_for(nx, ny, nz, o->eo);
+        CK(cudaFuncSetAttribute(contour_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 0;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, contour_kernel_f64, kContourThreads, smem));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, contour_fn, kContourThreads, smem));
         if (per_sm < 1) return SCFT_OK;
         const int units = 2 * (nx > ny ? nx : ny);
         persistent_grid = std::min(units, per_sm * sms);
@@ -367,7 +400,7 @@ struct scft_diblock_s {
         attr[0].val.cooperative = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        CK(cudaLaunchKernelEx(&cfg, contour_kernel_f64, a));
+        CK(cudaLaunchKernelEx(&cfg, contour_fn, a));
         return SCFT_OK;
     }
 
