@@ -75,7 +75,7 @@ def load(build_if_missing: bool = True):
     global _lib
     if _lib is not None:
         return _lib
-    path = _build.LIB
+    path = os.environ.get("CRYSSCFT_LIB", _build.LIB)  # alternative build (A/B comparisons)
     if build_if_missing and (not os.path.exists(path) or _build.needs_build()):
         if os.path.exists(_build.NVCC):
             _build.build()

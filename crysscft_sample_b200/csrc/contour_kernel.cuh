@@ -43,6 +43,7 @@ struct ContourArgs {
     unsigned* bar_count;    // zeroed by the host before each launch
     int* error;             // bit 0: barrier wait gave up
     long long spin_limit;
+    unsigned* flags;        // alternating kernel: [chain][plane|slab][unit] last finished phase + 1, zeroed by the host
 };
 
 __device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
@@ -73,7 +74,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned* count, int* error, unsign
                 ok = 0;
                 break;
             }
-            __nanosleep(32);
+            if (spins > 256) __nanosleep(32);
         }
         __threadfence();
         if (*((volatile int*)error) != 0) ok = 0;
@@ -603,6 +604,237 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_kernel_ct(const Co
             if (!grid_barrier(a.bar_count, a.error, target, a.spin_limit)) return;
         }
     }
+}
+
+}  // namespace crysscft
+
+// ---------------------------------------------------------------------------
+// Alternating-layout schedule (cubic grids): the three axis operators commute, so
+// the phase that finishes step k can also start step k+1 on the same data layout.
+//   plane phase (units (chain, x)):  [z y]  D  store q  D  [z y]  -> exchange buffer XP
+//   slab phase  (units (chain, y)):  [x]    D  store q  D  [x]    -> exchange buffer XS
+// Phase k (k = 0..U) finishes step k-1 (k >= 1) and starts step k (k < U); plane
+// phases have even k.  One grid barrier per step instead of two, and one exchange
+// round trip per step.  The Boltzmann-factor slices of the next phase are fetched
+// with cp.async before the barrier wait, so their latency hides behind it.
+// ---------------------------------------------------------------------------
+namespace crysscft {
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// N x N tile from global (row stride gs) into shared memory (row stride LF) with cp.async
+template <int N, int LF>
+__device__ __forceinline__ void tile_fetch(double* sm, const double* gm, long long gs) {
+    constexpr int PER_ROW = N / 2;
+    constexpr int TOTAL = N * PER_ROW;
+#pragma unroll 4
+    for (int e = threadIdx.x; e < TOTAL; e += kContourThreads) {
+        const int r = e / PER_ROW, c = (e - r * PER_ROW) * 2;
+        cp_async16(sm + r * LF + c, gm + r * gs + c);
+    }
+}
+
+// shared -> global copy of an N x N tile (row stride gs)
+template <int N, int LF>
+__device__ __forceinline__ void tile_store(const double* sm, double* gm, long long gs) {
+    constexpr int PER_ROW = N / 2;
+    constexpr int TOTAL = N * PER_ROW;
+#pragma unroll 4
+    for (int e = threadIdx.x; e < TOTAL; e += kContourThreads) {
+        const int r = e / PER_ROW, c = (e - r * PER_ROW) * 2;
+        *reinterpret_cast<double2*>(gm + r * gs + c) = *reinterpret_cast<const double2*>(sm + r * LF + c);
+    }
+}
+
+// T <- T * W (elementwise on an N x N tile in shared memory)
+template <int N, int LF>
+__device__ __forceinline__ void tile_scale(double* T, const double* W) {
+    constexpr int PER_ROW = N / 2;
+    constexpr int TOTAL = N * PER_ROW;
+#pragma unroll 4
+    for (int e = threadIdx.x; e < TOTAL; e += kContourThreads) {
+        const int r = e / PER_ROW, c = (e - r * PER_ROW) * 2;
+        double2 v = *reinterpret_cast<double2*>(T + r * LF + c);
+        const double2 w = *reinterpret_cast<const double2*>(W + r * LF + c);
+        v.x = v.x * w.x;
+        v.y = v.y * w.y;
+        *reinterpret_cast<double2*>(T + r * LF + c) = v;
+    }
+}
+
+// v = T * W0 stored to global (the finished q(s+1)); if start, T <- v * W1 (D of the next step)
+template <int N, int LF>
+__device__ __forceinline__ void tile_finish(double* T, const double* W0, const double* W1, double* gm,
+                                            long long gs, bool start) {
+    constexpr int PER_ROW = N / 2;
+    constexpr int TOTAL = N * PER_ROW;
+#pragma unroll 4
+    for (int e = threadIdx.x; e < TOTAL; e += kContourThreads) {
+        const int r = e / PER_ROW, c = (e - r * PER_ROW) * 2;
+        double2 v = *reinterpret_cast<double2*>(T + r * LF + c);
+        const double2 w0 = *reinterpret_cast<const double2*>(W0 + r * LF + c);
+        v.x = v.x * w0.x;
+        v.y = v.y * w0.y;
+        *reinterpret_cast<double2*>(gm + r * gs + c) = v;
+        if (start) {
+            const double2 w1 = *reinterpret_cast<const double2*>(W1 + r * LF + c);
+            v.x = v.x * w1.x;
+            v.y = v.y * w1.y;
+            *reinterpret_cast<double2*>(T + r * LF + c) = v;
+        }
+    }
+}
+
+template <int N, bool EO>
+struct AltShape {
+    static constexpr int LF = N + 4;
+    static constexpr int OPS = 3 * AxisShape<N, EO>::SIZE;
+    static constexpr int OPS_PAD = (OPS + 1) & ~1;
+    static constexpr int TILE = N * LF;
+    static constexpr size_t SMEM = (size_t)(OPS_PAD + 4 * TILE) * sizeof(double);
+};
+
+__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+template <int N, bool EO>
+__global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const ContourArgs a) {
+    using S = AltShape<N, EO>;
+    constexpr int LF = S::LF;
+    constexpr int OFFY = AxisShape<N, EO>::SIZE;
+    constexpr int OFFZ = 2 * AxisShape<N, EO>::SIZE;
+    constexpr int TPR = kContourThreads / N;         // threads per tile row (rows * TPR <= block)
+    constexpr int CPT = (N / 2 + TPR - 1) / TPR;     // 16-byte chunks per thread and row
+    static_assert(TPR >= 1, "tile rows must not exceed the block");
+    extern __shared__ __align__(16) double smem[];
+    double* sops = smem;
+    double* T0 = smem + S::OPS_PAD;
+    double* T1 = T0 + S::TILE;
+    double* W0 = T1 + S::TILE;  // D of the step being finished
+    double* W1 = W0 + S::TILE;  // D of the step being started
+    __shared__ int s_fail;
+    for (int i = threadIdx.x; i < S::OPS; i += kContourThreads) sops[i] = a.ops[i];
+    if (threadIdx.x == 0) s_fail = 0;
+
+    constexpr long long M = (long long)N * N * N;
+    constexpr long long PLANE = (long long)N * N;
+    const int units = a.nchain * N;
+    const int U = a.t_end;  // steps 0..U-1 of both chains (t_begin is 0)
+
+    // exp(-w ds/2) of step s of chain c: block A for segments < NsA, else block B
+    auto w_of = [&](int c, int s) -> const double* {
+        const int dir = c ? a.dir[1] : a.dir[0];
+        const long long in_slot = (c ? a.slot0[1] : a.slot0[0]) + (long long)dir * s;
+        const long long seg = dir > 0 ? in_slot : in_slot - 1;
+        return seg < a.NsA ? a.wds[0] : a.wds[1];
+    };
+    // cp.async the Boltzmann slices phase k of unit u needs (plane: x-plane; slab: y-row)
+    auto fetch_w = [&](int k, int u) {
+        const int c = u >= N ? 1 : 0, p = u - c * N;
+        const bool plane = (k & 1) == 0;
+        const long long off = plane ? (long long)p * PLANE : (long long)p * N;
+        const long long gs = plane ? N : PLANE;
+        if (k >= 1) tile_fetch<N, LF>(W0, w_of(c, k - 1) + off, gs);
+        if (k < U) tile_fetch<N, LF>(W1, w_of(c, k) + off, gs);
+        cp_async_commit();
+    };
+
+    if ((int)blockIdx.x < units) fetch_w(0, blockIdx.x);
+    for (int k = 0; k <= U; ++k) {
+        const bool plane = (k & 1) == 0;
+        for (int u = blockIdx.x; u < units; u += gridDim.x) {
+            const int c = u >= N ? 1 : 0, p = u - c * N;
+            const int dir = c ? a.dir[1] : a.dir[0];
+            const long long slot0 = c ? a.slot0[1] : a.slot0[0];
+            double* q = c ? a.q[1] : a.q[0];
+            double* XP = c ? a.xbuf[1] : a.xbuf[0];  // written by plane phases
+            double* XS = XP + M;                     // written by slab phases
+            unsigned* fl_plane = a.flags + (size_t)c * 2 * N;
+            unsigned* fl_slab = fl_plane + N;
+            const long long off = plane ? (long long)p * PLANE : (long long)p * N;
+            const long long gs = plane ? N : PLANE;
+            if (u != (int)blockIdx.x) fetch_w(k, u);  // more units than blocks
+            if (k == 0) {
+                tile_fetch<N, LF>(T0, q + slot0 * M + off, gs);
+            } else {
+                // row r of this tile was produced by unit r of the other layout in phase k-1:
+                // wait for its flag, then fetch the row (waits and copies overlap)
+                const int r = threadIdx.x / TPR, sub = threadIdx.x - r * TPR;
+                if (r < N) {
+                    const unsigned* f = plane ? fl_slab + r : fl_plane + r;
+                    long long spins = 0;
+                    while (ld_acquire_u32(f) < (unsigned)k) {
+                        if (++spins > a.spin_limit) {
+                            atomicOr(a.error, 1);
+                            s_fail = 1;
+                            break;
+                        }
+                        if (spins > 64) __nanosleep(20);
+                    }
+                    const double* src = (plane ? XS : XP) + off + r * gs;
+#pragma unroll
+                    for (int j = 0; j < CPT; ++j) {
+                        const int ch = sub + j * TPR;
+                        if (ch < N / 2) cp_async16(T0 + r * LF + 2 * ch, src + 2 * ch);
+                    }
+                }
+            }
+            cp_async_commit();
+            cp_async_wait_all();
+            __syncthreads();
+            if (s_fail) return;
+            double* cur = T0;
+            double* oth = T1;
+            if (k >= 1) {
+                // finish step k-1: the axis ops this layout owns, then D, store q
+                if (plane) {
+                    row_op_ct<N, N, LF, EO>(cur, oth, sops + OFFZ);
+                    __syncthreads();
+                    col_op_ct<N, N, LF, EO>(oth, cur, sops + OFFY);
+                } else {
+                    col_op_ct<N, N, LF, EO>(cur, oth, sops);
+                    double* tmp = cur;
+                    cur = oth;
+                    oth = tmp;
+                }
+                __syncthreads();
+                const long long out_slot = slot0 + (long long)dir * k;
+                tile_finish<N, LF>(cur, W0, W1, q + out_slot * M + off, gs, k < U);
+            } else {
+                tile_scale<N, LF>(cur, W1);
+            }
+            __syncthreads();
+            if (k < U) {
+                // start step k on this layout; the other layout finishes it next phase
+                if (plane) {
+                    row_op_ct<N, N, LF, EO>(cur, oth, sops + OFFZ);
+                    __syncthreads();
+                    col_op_ct<N, N, LF, EO>(oth, cur, sops + OFFY);
+                } else {
+                    col_op_ct<N, N, LF, EO>(cur, oth, sops);
+                    double* tmp = cur;
+                    cur = oth;
+                    oth = tmp;
+                }
+                __syncthreads();
+                tile_store<N, LF>(cur, (plane ? XP : XS) + off, gs);
+                __syncthreads();
+                if (threadIdx.x == 0) {
+                    __threadfence();
+                    st_release_u32((plane ? fl_plane : fl_slab) + p, (unsigned)(k + 1));
+                }
+            }
+            __syncthreads();
+        }
+        if (k < U && (int)blockIdx.x < units) fetch_w(k + 1, blockIdx.x);  // overlaps the next waits
+    }
+    cp_async_wait_all();
 }
 
 }  // namespace crysscft

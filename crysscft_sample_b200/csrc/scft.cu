@@ -183,6 +183,38 @@ cudaError_t launch_axis(const AxisPass<T>& p, int nchain, bool contiguous, cudaS
 
 using ContourFn = void (*)(const ContourArgs);
 
+// The alternating-layout contour kernel for cubic grids whose four tiles and operators
+// fit in shared memory; nullptr when there is none.
+ContourFn contour_alt_kernel_for(int n, int eo, size_t* smem) {
+#define CRYSSCFT_ALT(N, E)                     \
+    {                                          \
+        *smem = AltShape<N, E>::SMEM;          \
+        return contour_alt_kernel<N, E>;       \
+    }
+    if (eo) {
+        switch (n) {
+            case 16: CRYSSCFT_ALT(16, true)
+            case 32: CRYSSCFT_ALT(32, true)
+            case 48: CRYSSCFT_ALT(48, true)
+            case 64: CRYSSCFT_ALT(64, true)
+            default: break;
+        }
+    } else {
+        switch (n) {
+            case 8: CRYSSCFT_ALT(8, false)
+            case 16: CRYSSCFT_ALT(16, false)
+            case 24: CRYSSCFT_ALT(24, false)
+            case 32: CRYSSCFT_ALT(32, false)
+            case 40: CRYSSCFT_ALT(40, false)
+            case 48: CRYSSCFT_ALT(48, false)
+            case 56: CRYSSCFT_ALT(56, false)
+            default: break;
+        }
+    }
+#undef CRYSSCFT_ALT
+    return nullptr;
+}
+
 // The compile-time specialised contour kernel for cubic grids (all axes even/odd, or
 // all full), else the runtime-generic one.
 ContourFn contour_kernel_for(int nx, int ny, int nz, const int eo[3]) {
@@ -320,6 +352,10 @@ struct scft_diblock_s {
     int persistent_grid = 0;
     size_t persistent_smem = 0;
     ContourFn contour_fn = nullptr;
+    bool alternating = false;             // contour_fn is the alternating-layout kernel
+    bool no_alternating = false;          // force the two-phase schedule (A/B comparisons)
+    DevBuf<double> d_xch;                 // exchange buffers, 2 x space_size_phy per chain
+    DevBuf<unsigned> flags;               // per-unit phase flags of the alternating kernel
     DevBuf<unsigned> ctrl;                // [0] barrier arrivals, [1] error bits
     long long spin_limit = 20000000LL;
 
@@ -341,12 +377,24 @@ struct scft_diblock_s {
         }
         const int nx = (int)solver->grid_phy[0], ny = (int)solver->grid_phy[1], nz = (int)solver->grid_phy[2];
         const int rows = nx > ny ? nx : ny;
-        const size_t smem = ((size_t)((o->total + 1) & ~1) + 2 * (size_t)rows * (nz + 4)) * sizeof(double);
+        size_t smem = ((size_t)((o->total + 1) & ~1) + 2 * (size_t)rows * (nz + 4)) * sizeof(double);
         int dev_smem = 0, sms = 0;
         CK(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, solver->device));
         CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, solver->device));
         if (smem > (size_t)dev_smem) return SCFT_OK;
         contour_fn = contour_kernel_for(nx, ny, nz, o->eo);
+        alternating = false;
+        if (nx == ny && ny == nz && o->eo[0] == o->eo[1] && o->eo[1] == o->eo[2] && !no_alternating) {
+            size_t alt_smem = 0;
+            ContourFn f = contour_alt_kernel_for(nx, o->eo[0], &alt_smem);
+            if (f && alt_smem <= (size_t)dev_smem) {
+                contour_fn = f;
+                smem = alt_smem;
+                alternating = true;
+            }
+        }
+        if (!d_xch.p) CKR(d_xch.alloc(4 * M));
+        if (alternating && flags.n != (size_t)(4 * nx)) CKR(flags.alloc((size_t)4 * nx));
         CK(cudaFuncSetAttribute(contour_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 0;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, contour_fn, kContourThreads, smem));
@@ -367,8 +415,8 @@ struct scft_diblock_s {
         a.q[1] = qc;
         a.wds[0] = wAds;
         a.wds[1] = wBds;
-        a.xbuf[0] = d_t[0].p;
-        a.xbuf[1] = d_t[1].p;
+        a.xbuf[0] = d_xch.p;          // 2M per chain: plane- and slab-phase exchange buffers
+        a.xbuf[1] = d_xch.p + 2 * M;
         a.ops = o->d_packed.p;
         for (int ax = 0; ax < 3; ++ax) {
             a.n[ax] = (int)solver->grid_phy[ax];
@@ -389,7 +437,9 @@ struct scft_diblock_s {
         a.bar_count = ctrl.p;
         a.error = reinterpret_cast<int*>(ctrl.p + 1);
         a.spin_limit = spin_limit;
+        a.flags = flags.p;
         CK(cudaMemsetAsync(ctrl.p, 0, sizeof(unsigned), st));
+        if (alternating) CK(cudaMemsetAsync(flags.p, 0, flags.n * sizeof(unsigned), st));
         cudaLaunchConfig_t cfg{};
         cfg.gridDim = dim3((unsigned)persistent_grid);
         cfg.blockDim = dim3(kContourThreads);
