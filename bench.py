@@ -185,20 +185,11 @@ def run_ours(args):
     import numpy as np
     import torch
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from crysscft_sample_b200 import fields, replicas, scft, solvers
+
+    rank, world, local = replicas.dist_env()
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-
-    from crysscft_sample_b200 import fields, scft, solvers
+    dist = replicas.init("nccl", timeout_s=120)
 
     n = args.grid
     N = (n, n, n)
@@ -215,16 +206,11 @@ def run_ours(args):
     U = run.NsA + run.NsB
 
     def barrier():
-        if dist is not None:
-            dist.barrier()
+        replicas.barrier(dist)
         torch.cuda.synchronize()
 
     def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(dist, x)
 
     # ---- device-resident timed region ------------------------------------
     run.iterate(max(args.warmup, 3))

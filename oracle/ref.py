@@ -78,6 +78,23 @@ def _p(a: np.ndarray):
     return a.ctypes.data_as(_dp)
 
 
+def check_grid(kind: str, grid_log) -> None:
+    """The reference constructors print "ERROR" and call exit(1) on these grids
+    (src/solver_p1.h:101-108, src/solver_3m.h:81-92, src/solver_Pmmm.h:71-82);
+    refuse them here so the calling process survives."""
+    Nx, Ny, Nz = (int(v) for v in grid_log)
+    if min(Nx, Ny, Nz) <= 0:
+        raise ValueError("ERROR: Bad Grid Size")
+    if kind == "P1":
+        if Nz % 8:
+            raise ValueError("ERROR: Bad Grid Size For Group Triclinic P1, alignment cannot be guaranteed")
+    else:
+        if Nx % 2 or Ny % 2 or Nz % 2:
+            raise ValueError("ERROR: Grid Size Must Be Even")
+        if (Nz // 2) % 8:
+            raise ValueError("ERROR: Bad Grid Size, Alignment Cannot Be Guaranteed")
+
+
 def set_num_threads(n: int) -> None:
     lib().ref_set_num_threads(int(n))
 
@@ -91,6 +108,7 @@ class RefSolver:
 
     def __init__(self, kind: str, grid_log, translational_part=None):
         self.kind = kind.upper()
+        check_grid(self.kind, grid_log)
         g = None
         if translational_part is not None:
             self._g = np.ascontiguousarray(translational_part, dtype=np.float64)
