@@ -234,11 +234,21 @@ def run_ours(args):
 
     # ---- phase timer: the triplet kernels' share (roofline) ---------------
     phases = run.time_phases(10)
-    chain_ms = phases[1]
+    chain_s = phases[1] / 1e3  # one launch of the contour kernel = all 2U triplets of an iteration
     b = 8 if args.precision == "fp64" else 4
-    alg_bytes_step = 2 * 3 * M * b  # both chains: read q(s), read exp(-w ds/2), write q(s+1)
-    step_s = chain_ms / 1e3 / U
-    achieved = alg_bytes_step / step_s / 1e9
+    # per triplet: read q(s), read exp(-w ds/2), write q(s+1); K generated on chip, not counted
+    alg_bytes_launch = 2 * U * 3 * M * b
+    achieved = alg_bytes_launch / chain_s / 1e9
+    # FP64 multiply-adds of the triplets: per point and axis n/2 (even/odd operators) or n
+    n_phy = solver.get_grid_size_phy()
+    per_point = sum((v // 2) if (args.solver != "3M" and v % 16 == 0) else v for v in n_phy)
+    flops_launch = 2.0 * 2 * U * M * per_point
+    import ctypes as _ct
+
+    from crysscft_sample_b200 import _lib as _L
+
+    simt, tens = _ct.c_double(), _ct.c_double()
+    _L.check(_L.load().scft_measure_fp64_peak(local, _ct.byref(simt), _ct.byref(tens)))
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -251,7 +261,7 @@ def run_ours(args):
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
             tj = json.load(f)
         key = f"{args.solver}_{args.precision}_{n}"
-        traffic = tj.get(key, {}).get("bytes_per_step")
+        traffic = tj.get(key, {}).get("dram_bytes_per_launch")
     except Exception:
         pass
 
@@ -288,9 +298,15 @@ def run_ours(args):
                                         "fields_energy": phases[3]},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "triplet step (z, y, x axis passes; both chains)",
+                         "kernel": "contour kernel: one launch = the 2 x 200 triplets of one iteration",
+                         "algorithmic_bytes_per_launch": alg_bytes_launch,
+                         "launch_ms": chain_s * 1e3,
                          "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured"
-                         else "fallback 6650 GB/s"},
+                         else "fallback 6650 GB/s",
+                         "fp64": {"achieved_tflops": flops_launch / chain_s / 1e12,
+                                  "peak_tflops": tens.value, "peak_simt_tflops": simt.value,
+                                  "frac": flops_launch / chain_s / 1e12 / tens.value,
+                                  "peak_source": "measured live (scft_measure_fp64_peak, FP64 m8n8k4 MMA)"}},
             "e2e": {"value": e2e_value, "unit": "iterations/s", "h2d_bytes_per_step": 2 * M * 8,
                     "d2h_bytes_per_step": 4 * M * 8 + 8 * 8},
             "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"],

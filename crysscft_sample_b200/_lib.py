@@ -53,6 +53,7 @@ SIGNATURES = {
     "scft_diblock_time_phases": (ctypes.c_int, [_vp, _sz, _dp]),
     "scft_solver_set_stream": (ctypes.c_int, [_vp, _vp]),
     "scft_solver_diffusion_device_static_scratch": (ctypes.c_int, [_vp, _vp, _vp]),
+    "scft_measure_fp64_peak": (ctypes.c_int, [ctypes.c_int, _dp, _dp]),
 }
 
 _lib = None

@@ -167,6 +167,11 @@ int scft_diblock_time_phases(scft_diblock_t d, size_t n_iter, double out[4]);
 #define SCFT_STATIC_SCRATCH_MAX_POINTS 262144
 int scft_solver_diffusion_device_static_scratch(scft_solver_t solver, double* d_io, void* stream);
 
+/* Measured FP64 throughput of `device` in TFLOP/s: FMA on the CUDA cores and
+ * m8n8k4 MMA on the tensor cores (the denominator of the FP64 roofline).  No
+ * counterpart in the reference (it has no GPU path). */
+int scft_measure_fp64_peak(int device, double* tflops_simt, double* tflops_tensor);
+
 /* Make the solver (and every diblock built on it) issue its work on `stream`
  * (a cudaStream_t; NULL restores the solver's own stream). */
 int scft_solver_set_stream(scft_solver_t solver, void* stream);

@@ -26,11 +26,36 @@ _lib = None
 _dp = ctypes.POINTER(ctypes.c_double)
 
 
+GPU_DRIVER_PATH = os.path.join(_HERE, "_ref", "libref_gpu_driver.so")
+
+
 def build(ref_src: str = "/root/reference/src") -> None:
-    """Compile oracle/_ref/ from the reference sources (only where they exist)."""
+    """Compile oracle/_ref/ from the reference sources (only where they exist); the
+    reference-driver-over-GPU-adapters library too when the CUDA library is built."""
     if not os.path.isdir(ref_src):
         return
-    subprocess.run(["make", "-s", "-C", _HERE, f"REF_SRC={ref_src}", "all", "shim"], check=True)
+    targets = ["all", "shim"]
+    gpulib = os.path.join(os.path.dirname(_HERE), "crysscft_sample_b200", "_lib", "libcrysscft_b200.so")
+    if os.path.exists(gpulib):
+        targets.append("gpu_driver")
+    subprocess.run(["make", "-s", "-C", _HERE, f"REF_SRC={ref_src}"] + targets, check=True)
+
+
+def run_reference_driver_on_gpu(kind: str, grid_log, fA, ds, xN, L, acceptance, nstep, wA0, wB0, name: str) -> str:
+    """The reference's unmodified diblock_scft_simple_iterate over the GPU solver adapters
+    (include/crysscft_b200_solvers.hpp); returns what the driver prints."""
+    check_grid(kind.upper(), grid_log)
+    G = ctypes.CDLL(GPU_DRIVER_PATH)
+    G.refgpu_run_driver.restype = ctypes.c_long
+    G.refgpu_run_driver.argtypes = ([ctypes.c_int] + [ctypes.c_long] * 3 + [ctypes.c_double] * 7
+                                    + [ctypes.c_long, _dp, _dp, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_long])
+    buf = ctypes.create_string_buffer(1 << 16)
+    wA0 = np.ascontiguousarray(wA0, dtype=np.float64).ravel()
+    wB0 = np.ascontiguousarray(wB0, dtype=np.float64).ravel()
+    nx, ny, nz = (int(v) for v in grid_log)
+    G.refgpu_run_driver(KINDS[kind.upper()], nx, ny, nz, fA, ds, xN, L[0], L[1], L[2], acceptance, int(nstep),
+                        _p(wA0), _p(wB0), name.encode(), buf, len(buf))
+    return buf.value.decode()
 
 
 def available() -> bool:
