@@ -1,0 +1,417 @@
+// FP32 form of the alternating-layout contour kernel (precision form of the triplets).
+//
+// Same schedule as contour_alt_kernel (plane phases [A_z A_y], slab phases [A_x],
+// per-unit release flags, cp.async prefetch), with FP32 contour slices and
+// Boltzmann factors.  The axis products run on the tensor cores as 3xTF32 split
+// products (mma.sync m16n8k8 .tf32, FP32 accumulate): every operand x is split
+// into hi = tf32(x) and lo = tf32(x - hi) and a*b ~ a_lo b_hi + a_hi b_lo + a_hi b_hi,
+// which keeps FP32-level accuracy (the dropped a_lo b_lo term is ~2^-22 relative).
+// Operators are split on the host; field values are split on the fly.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "contour_kernel.cuh"
+
+namespace crysscft {
+
+__device__ __forceinline__ unsigned f32_to_tf32(float x) {
+    unsigned r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ void split_tf32(float x, unsigned& hi, unsigned& lo) {
+    hi = f32_to_tf32(x);
+    lo = f32_to_tf32(x - __uint_as_float(hi));
+}
+__device__ __forceinline__ void mma_tf32(float (&d)[4], unsigned a0, unsigned a1, unsigned a2, unsigned a3,
+                                         unsigned b0, unsigned b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+// d += (ahi + alo)(bhi + blo) without the lo*lo term, small terms first
+__device__ __forceinline__ void mma_3xtf32(float (&d)[4], const unsigned (&ah)[4], const unsigned (&al)[4],
+                                           const unsigned (&bh)[2], const unsigned (&bl)[2]) {
+    mma_tf32(d, al[0], al[1], al[2], al[3], bh[0], bh[1]);
+    mma_tf32(d, ah[0], ah[1], ah[2], ah[3], bl[0], bl[1]);
+    mma_tf32(d, ah[0], ah[1], ah[2], ah[3], bh[0], bh[1]);
+}
+
+// Per-axis operator block in FP32: [hi part][lo part], each E then O (even/odd) or A (full).
+template <int N, bool EO>
+struct AxisShapeF {
+    static constexpr int K = EO ? N / 2 : N;
+    static constexpr int LD = K + 4;
+    static constexpr int HALF = EO ? K * LD : 0;            // E -> O
+    static constexpr int PART = EO ? 2 * K * LD : N * LD;   // hi -> lo
+    static constexpr int SIZE = 2 * PART;
+};
+
+// G[r][i] = sum_j F[r][j] A[i][j] on an R x C slab: m16 tiles over r, n8 tiles over i
+template <int R, int C, int LF, bool EO>
+__device__ __forceinline__ void row_op_f32(const float* __restrict__ F, float* __restrict__ G,
+                                           const float* __restrict__ op) {
+    using S = AxisShapeF<C, EO>;
+    constexpr int NI = S::K, K = S::K, LD = S::LD;
+    constexpr int TM = R / 16, TN = NI / 8;
+    constexpr int BN = (TN + 1) / 2;  // blocks of 1 x 2 tiles
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll 1
+    for (int blk = warp; blk < TM * BN; blk += kContourThreads / 32) {
+        const int m0 = (blk / BN) * 16, nb = (blk % BN) * 2;
+        const bool n1 = (TN % 2 == 0) || (nb + 1 < TN);
+        float dP[2][4] = {}, dR[2][4] = {};
+        const float* Fr0 = F + (m0 + g) * LF;
+        const float* Fr1 = Fr0 + 8 * LF;
+#pragma unroll
+        for (int k0 = 0; k0 < K; k0 += 8) {
+            unsigned uh[4], ul[4], vh[4], vl[4];
+            {
+                const int j0 = k0 + t, j1 = k0 + t + 4;
+                const float x[4] = {Fr0[j0], Fr1[j0], Fr0[j1], Fr1[j1]};
+                if (EO) {
+                    const float y[4] = {Fr0[C - 1 - j0], Fr1[C - 1 - j0], Fr0[C - 1 - j1], Fr1[C - 1 - j1]};
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        split_tf32(x[e] + y[e], uh[e], ul[e]);
+                        split_tf32(x[e] - y[e], vh[e], vl[e]);
+                    }
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) split_tf32(x[e], uh[e], ul[e]);
+                }
+            }
+#pragma unroll
+            for (int b = 0; b < 2; ++b) {
+                if (b == 1 && !n1) continue;
+                const int i = (nb + b) * 8 + g;
+                const float* Eh = op + i * LD + k0 + t;
+                const float* El = Eh + S::PART;
+                unsigned bh[2] = {__float_as_uint(Eh[0]), __float_as_uint(Eh[4])};
+                unsigned bl[2] = {__float_as_uint(El[0]), __float_as_uint(El[4])};
+                mma_3xtf32(dP[b], uh, ul, bh, bl);
+                if (EO) {
+                    const float* Oh = Eh + S::HALF;
+                    const float* Ol = El + S::HALF;
+                    unsigned ch[2] = {__float_as_uint(Oh[0]), __float_as_uint(Oh[4])};
+                    unsigned cl[2] = {__float_as_uint(Ol[0]), __float_as_uint(Ol[4])};
+                    mma_3xtf32(dR[b], vh, vl, ch, cl);
+                }
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            if (b == 1 && !n1) continue;
+            const int i = (nb + b) * 8 + 2 * t;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int r = m0 + g + 8 * h;
+                const float p0 = dP[b][2 * h], p1 = dP[b][2 * h + 1];
+                if (EO) {
+                    const float r0 = dR[b][2 * h], r1 = dR[b][2 * h + 1];
+                    *reinterpret_cast<float2*>(G + r * LF + i) = make_float2(p0 + r0, p1 + r1);
+                    *reinterpret_cast<float2*>(G + r * LF + (C - 2 - i)) = make_float2(p1 - r1, p0 - r0);
+                } else {
+                    *reinterpret_cast<float2*>(G + r * LF + i) = make_float2(p0, p1);
+                }
+            }
+        }
+    }
+}
+
+// G[i][c] = sum_j A[i][j] F[j][c] on an R x C slab: m16 tiles over i, n8 tiles over c
+template <int R, int C, int LF, bool EO>
+__device__ __forceinline__ void col_op_f32(const float* __restrict__ F, float* __restrict__ G,
+                                           const float* __restrict__ op) {
+    using S = AxisShapeF<R, EO>;
+    constexpr int MI = S::K, K = S::K, LD = S::LD;
+    constexpr int TM = MI / 16, TN = C / 8;
+    constexpr int BN = (TN + 1) / 2;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll 1
+    for (int blk = warp; blk < TM * BN; blk += kContourThreads / 32) {
+        const int m0 = (blk / BN) * 16, nb = (blk % BN) * 2;
+        const bool n1 = (TN % 2 == 0) || (nb + 1 < TN);
+        float dP[2][4] = {}, dR[2][4] = {};
+        const float* Eh0 = op + (m0 + g) * LD + t;
+        const float* Eh1 = Eh0 + 8 * LD;
+#pragma unroll
+        for (int k0 = 0; k0 < K; k0 += 8) {
+            unsigned ah[4] = {__float_as_uint(Eh0[k0]), __float_as_uint(Eh1[k0]), __float_as_uint(Eh0[k0 + 4]),
+                              __float_as_uint(Eh1[k0 + 4])};
+            unsigned al[4] = {__float_as_uint(Eh0[k0 + S::PART]), __float_as_uint(Eh1[k0 + S::PART]),
+                              __float_as_uint(Eh0[k0 + 4 + S::PART]), __float_as_uint(Eh1[k0 + 4 + S::PART])};
+            unsigned oh[4], ol[4];
+            if (EO) {
+                oh[0] = __float_as_uint(Eh0[k0 + S::HALF]);
+                oh[1] = __float_as_uint(Eh1[k0 + S::HALF]);
+                oh[2] = __float_as_uint(Eh0[k0 + 4 + S::HALF]);
+                oh[3] = __float_as_uint(Eh1[k0 + 4 + S::HALF]);
+                ol[0] = __float_as_uint(Eh0[k0 + S::HALF + S::PART]);
+                ol[1] = __float_as_uint(Eh1[k0 + S::HALF + S::PART]);
+                ol[2] = __float_as_uint(Eh0[k0 + 4 + S::HALF + S::PART]);
+                ol[3] = __float_as_uint(Eh1[k0 + 4 + S::HALF + S::PART]);
+            }
+#pragma unroll
+            for (int b = 0; b < 2; ++b) {
+                if (b == 1 && !n1) continue;
+                const int c = (nb + b) * 8 + g;
+                const int j0 = k0 + t, j1 = k0 + t + 4;
+                const float x0 = F[j0 * LF + c], x1 = F[j1 * LF + c];
+                unsigned uh[2], ul[2];
+                if (EO) {
+                    const float y0 = F[(R - 1 - j0) * LF + c], y1 = F[(R - 1 - j1) * LF + c];
+                    unsigned vh[2], vl[2];
+                    split_tf32(x0 + y0, uh[0], ul[0]);
+                    split_tf32(x1 + y1, uh[1], ul[1]);
+                    split_tf32(x0 - y0, vh[0], vl[0]);
+                    split_tf32(x1 - y1, vh[1], vl[1]);
+                    mma_3xtf32(dP[b], ah, al, uh, ul);
+                    mma_3xtf32(dR[b], oh, ol, vh, vl);
+                } else {
+                    split_tf32(x0, uh[0], ul[0]);
+                    split_tf32(x1, uh[1], ul[1]);
+                    mma_3xtf32(dP[b], ah, al, uh, ul);
+                }
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            if (b == 1 && !n1) continue;
+            const int c = (nb + b) * 8 + 2 * t;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int i = m0 + g + 8 * h;
+                const float p0 = dP[b][2 * h], p1 = dP[b][2 * h + 1];
+                if (EO) {
+                    const float r0 = dR[b][2 * h], r1 = dR[b][2 * h + 1];
+                    *reinterpret_cast<float2*>(G + i * LF + c) = make_float2(p0 + r0, p1 + r1);
+                    *reinterpret_cast<float2*>(G + (R - 1 - i) * LF + c) = make_float2(p0 - r0, p1 - r1);
+                } else {
+                    *reinterpret_cast<float2*>(G + i * LF + c) = make_float2(p0, p1);
+                }
+            }
+        }
+    }
+}
+
+// ---- N x N FP32 tiles between global (row stride gs) and shared memory (row stride LF)
+template <int N, int LF>
+__device__ __forceinline__ void tile_fetch_f32(float* sm, const float* gm, long long gs) {
+    constexpr int PER_ROW = N / 4;
+    constexpr int TOTAL = N * PER_ROW;
+#pragma unroll 4
+    for (int e = threadIdx.x; e < TOTAL; e += kContourThreads) {
+        const int r = e / PER_ROW, c = (e - r * PER_ROW) * 4;
+        cp_async16(sm + r * LF + c, gm + r * gs + c);
+    }
+}
+template <int N, int LF>
+__device__ __forceinline__ void tile_store_f32(const float* sm, float* gm, long long gs) {
+    constexpr int PER_ROW = N / 4;
+    constexpr int TOTAL = N * PER_ROW;
+#pragma unroll 4
+    for (int e = threadIdx.x; e < TOTAL; e += kContourThreads) {
+        const int r = e / PER_ROW, c = (e - r * PER_ROW) * 4;
+        *reinterpret_cast<float4*>(gm + r * gs + c) = *reinterpret_cast<const float4*>(sm + r * LF + c);
+    }
+}
+template <int N, int LF>
+__device__ __forceinline__ void tile_scale_f32(float* T, const float* W) {
+    constexpr int PER_ROW = N / 4;
+    constexpr int TOTAL = N * PER_ROW;
+#pragma unroll 4
+    for (int e = threadIdx.x; e < TOTAL; e += kContourThreads) {
+        const int r = e / PER_ROW, c = (e - r * PER_ROW) * 4;
+        float4 v = *reinterpret_cast<float4*>(T + r * LF + c);
+        const float4 w = *reinterpret_cast<const float4*>(W + r * LF + c);
+        v.x *= w.x;
+        v.y *= w.y;
+        v.z *= w.z;
+        v.w *= w.w;
+        *reinterpret_cast<float4*>(T + r * LF + c) = v;
+    }
+}
+template <int N, int LF>
+__device__ __forceinline__ void tile_finish_f32(float* T, const float* W0, const float* W1, float* gm, long long gs,
+                                                bool start) {
+    constexpr int PER_ROW = N / 4;
+    constexpr int TOTAL = N * PER_ROW;
+#pragma unroll 4
+    for (int e = threadIdx.x; e < TOTAL; e += kContourThreads) {
+        const int r = e / PER_ROW, c = (e - r * PER_ROW) * 4;
+        float4 v = *reinterpret_cast<float4*>(T + r * LF + c);
+        const float4 w0 = *reinterpret_cast<const float4*>(W0 + r * LF + c);
+        v.x *= w0.x;
+        v.y *= w0.y;
+        v.z *= w0.z;
+        v.w *= w0.w;
+        *reinterpret_cast<float4*>(gm + r * gs + c) = v;
+        if (start) {
+            const float4 w1 = *reinterpret_cast<const float4*>(W1 + r * LF + c);
+            v.x *= w1.x;
+            v.y *= w1.y;
+            v.z *= w1.z;
+            v.w *= w1.w;
+            *reinterpret_cast<float4*>(T + r * LF + c) = v;
+        }
+    }
+}
+
+template <int N, bool EO>
+struct AltShapeF {
+    static constexpr int LF = N + 4;
+    static constexpr int OPS = 3 * AxisShapeF<N, EO>::SIZE;
+    static constexpr int OPS_PAD = (OPS + 3) & ~3;
+    static constexpr int TILE = N * LF;
+    static constexpr size_t SMEM = (size_t)(OPS_PAD + 4 * TILE) * sizeof(float);
+};
+
+struct ContourArgsF {
+    float* q[2];
+    const float* wds[2];
+    float* xbuf[2];        // 2 x space_size_phy per chain
+    const float* ops;      // packed FP32 operators (hi/lo), x then y then z
+    int nchain;
+    long long slot0[2];
+    int dir[2];
+    long long NsA;
+    int t_end;
+    int* error;
+    long long spin_limit;
+    unsigned* flags;       // [chain][plane|slab][unit], zeroed by the host
+};
+
+template <int N, bool EO>
+__global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel_f32(const ContourArgsF a) {
+    using S = AltShapeF<N, EO>;
+    constexpr int LF = S::LF;
+    constexpr int OFFY = AxisShapeF<N, EO>::SIZE;
+    constexpr int OFFZ = 2 * AxisShapeF<N, EO>::SIZE;
+    constexpr int TPR = kContourThreads / N;
+    constexpr int CPT = (N / 4 + TPR - 1) / TPR;
+    static_assert(TPR >= 1, "tile rows must not exceed the block");
+    extern __shared__ __align__(16) float smemf[];
+    float* sops = smemf;
+    float* T0 = smemf + S::OPS_PAD;
+    float* T1 = T0 + S::TILE;
+    float* W0 = T1 + S::TILE;
+    float* W1 = W0 + S::TILE;
+    __shared__ int s_fail;
+    for (int i = threadIdx.x; i < S::OPS; i += kContourThreads) sops[i] = a.ops[i];
+    if (threadIdx.x == 0) s_fail = 0;
+
+    constexpr long long M = (long long)N * N * N;
+    constexpr long long PLANE = (long long)N * N;
+    const int units = a.nchain * N;
+    const int U = a.t_end;
+
+    auto w_of = [&](int c, int s) -> const float* {
+        const int dir = c ? a.dir[1] : a.dir[0];
+        const long long in_slot = (c ? a.slot0[1] : a.slot0[0]) + (long long)dir * s;
+        const long long seg = dir > 0 ? in_slot : in_slot - 1;
+        return seg < a.NsA ? a.wds[0] : a.wds[1];
+    };
+    auto fetch_w = [&](int k, int u) {
+        const int c = u >= N ? 1 : 0, p = u - c * N;
+        const bool plane = (k & 1) == 0;
+        const long long off = plane ? (long long)p * PLANE : (long long)p * N;
+        const long long gs = plane ? N : PLANE;
+        if (k >= 1) tile_fetch_f32<N, LF>(W0, w_of(c, k - 1) + off, gs);
+        if (k < U) tile_fetch_f32<N, LF>(W1, w_of(c, k) + off, gs);
+        cp_async_commit();
+    };
+
+    if ((int)blockIdx.x < units) fetch_w(0, blockIdx.x);
+    for (int k = 0; k <= U; ++k) {
+        const bool plane = (k & 1) == 0;
+        for (int u = blockIdx.x; u < units; u += gridDim.x) {
+            const int c = u >= N ? 1 : 0, p = u - c * N;
+            const int dir = c ? a.dir[1] : a.dir[0];
+            const long long slot0 = c ? a.slot0[1] : a.slot0[0];
+            float* q = c ? a.q[1] : a.q[0];
+            float* XP = c ? a.xbuf[1] : a.xbuf[0];
+            float* XS = XP + M;
+            unsigned* fl_plane = a.flags + (size_t)c * 2 * N;
+            unsigned* fl_slab = fl_plane + N;
+            const long long off = plane ? (long long)p * PLANE : (long long)p * N;
+            const long long gs = plane ? N : PLANE;
+            if (u != (int)blockIdx.x) fetch_w(k, u);
+            if (k == 0) {
+                tile_fetch_f32<N, LF>(T0, q + slot0 * M + off, gs);
+            } else {
+                const int r = threadIdx.x / TPR, sub = threadIdx.x - r * TPR;
+                if (r < N) {
+                    const unsigned* f = plane ? fl_slab + r : fl_plane + r;
+                    long long spins = 0;
+                    while (ld_acquire_u32(f) < (unsigned)k) {
+                        if (++spins > a.spin_limit) {
+                            atomicOr(a.error, 1);
+                            s_fail = 1;
+                            break;
+                        }
+                        if (spins > 64) __nanosleep(20);
+                    }
+                    const float* src = (plane ? XS : XP) + off + r * gs;
+#pragma unroll
+                    for (int j = 0; j < CPT; ++j) {
+                        const int ch = sub + j * TPR;
+                        if (ch < N / 4) cp_async16(T0 + r * LF + 4 * ch, src + 4 * ch);
+                    }
+                }
+            }
+            cp_async_commit();
+            cp_async_wait_all();
+            __syncthreads();
+            if (s_fail) return;
+            float* cur = T0;
+            float* oth = T1;
+            if (k >= 1) {
+                if (plane) {
+                    row_op_f32<N, N, LF, EO>(cur, oth, sops + OFFZ);
+                    __syncthreads();
+                    col_op_f32<N, N, LF, EO>(oth, cur, sops + OFFY);
+                } else {
+                    col_op_f32<N, N, LF, EO>(cur, oth, sops);
+                    float* tmp = cur;
+                    cur = oth;
+                    oth = tmp;
+                }
+                __syncthreads();
+                const long long out_slot = slot0 + (long long)dir * k;
+                tile_finish_f32<N, LF>(cur, W0, W1, q + out_slot * M + off, gs, k < U);
+            } else {
+                tile_scale_f32<N, LF>(cur, W1);
+            }
+            __syncthreads();
+            if (k < U) {
+                if (plane) {
+                    row_op_f32<N, N, LF, EO>(cur, oth, sops + OFFZ);
+                    __syncthreads();
+                    col_op_f32<N, N, LF, EO>(oth, cur, sops + OFFY);
+                } else {
+                    col_op_f32<N, N, LF, EO>(cur, oth, sops);
+                    float* tmp = cur;
+                    cur = oth;
+                    oth = tmp;
+                }
+                __syncthreads();
+                tile_store_f32<N, LF>(cur, (plane ? XP : XS) + off, gs);
+                __syncthreads();
+                if (threadIdx.x == 0) {
+                    __threadfence();
+                    st_release_u32((plane ? fl_plane : fl_slab) + p, (unsigned)(k + 1));
+                }
+            }
+            __syncthreads();
+        }
+        if (k < U && (int)blockIdx.x < units) fetch_w(k + 1, blockIdx.x);
+    }
+    cp_async_wait_all();
+}
+
+}  // namespace crysscft

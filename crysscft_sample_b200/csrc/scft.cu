@@ -18,6 +18,7 @@
 #include "../../include/crysscft_b200.h"
 #include "axis_kernels.cuh"
 #include "contour_kernel.cuh"
+#include "contour_kernel_f32.cuh"
 #include "field_kernels.cuh"
 #include "operators.h"
 
@@ -82,7 +83,58 @@ struct OpsSet {
     DevBuf<double> d_packed;
     int eo[3] = {0, 0, 0}, off[3] = {0, 0, 0}, ld[3] = {0, 0, 0}, half[3] = {0, 0, 0};
     int total = 0;
+    // FP32 precision form: per axis [hi][lo] TF32 split parts, each E,O (even/odd) or A
+    std::vector<float> h_packed_f32;
+    DevBuf<float> f_packed;
+    int eo_f32[3] = {0, 0, 0};
 };
+
+// Round an FP32 value to the TF32 format (10 explicit mantissa bits), to nearest with
+// ties away from zero; the result is an FP32 value whose low 13 mantissa bits are 0.
+float round_to_tf32(float x) {
+    uint32_t u;
+    std::memcpy(&u, &x, sizeof(u));
+    if ((u & 0x7f800000u) != 0x7f800000u) {
+        u += 0x1000u;
+        u &= 0xffffe000u;
+    }
+    float r;
+    std::memcpy(&r, &u, sizeof(r));
+    return r;
+}
+
+// Append one axis operator to the FP32 packed buffer as TF32 hi/lo parts:
+// hi = tf32(a), lo = tf32(a - hi) evaluated from the long double value.
+void pack_operator_f32(const std::vector<long double>& A, int n, OpsSet& s, int axis) {
+    bool centro = (n % 32 == 0);
+    for (int i = 0; centro && i < n; ++i)
+        for (int j = 0; j < n; ++j) {
+            const long double a = A[(size_t)i * n + j], b = A[(size_t)(n - 1 - i) * n + (n - 1 - j)];
+            if (fabsl(a - b) > 1e-17L * (1.0L + fabsl(a))) { centro = false; break; }
+        }
+    s.eo_f32[axis] = centro ? 1 : 0;
+    const int K = centro ? n / 2 : n, ld = K + 4;
+    const size_t part = centro ? 2 * (size_t)K * ld : (size_t)n * ld;
+    const size_t base = s.h_packed_f32.size();
+    s.h_packed_f32.resize(base + 2 * part, 0.0f);
+    float* hi = s.h_packed_f32.data() + base;
+    float* lo = hi + part;
+    auto put = [&](size_t idx, long double v) {
+        const float h = round_to_tf32((float)v);
+        hi[idx] = h;
+        lo[idx] = round_to_tf32((float)(v - (long double)h));
+    };
+    for (int i = 0; i < (centro ? K : n); ++i)
+        for (int j = 0; j < K; ++j) {
+            if (centro) {
+                const long double a = A[(size_t)i * n + j], b = A[(size_t)i * n + (n - 1 - j)];
+                put((size_t)i * ld + j, (a + b) / 2);
+                put((size_t)K * ld + (size_t)i * ld + j, (a - b) / 2);
+            } else {
+                put((size_t)i * ld + j, A[(size_t)i * n + j]);
+            }
+        }
+}
 
 // Append one axis operator to the packed buffer, in even/odd form when A is
 // centrosymmetric (A[n-1-i][n-1-j] == A[i][j]) and n is a multiple of 16.
@@ -185,6 +237,34 @@ using ContourFn = void (*)(const ContourArgs);
 
 // The alternating-layout contour kernel for cubic grids whose four tiles and operators
 // fit in shared memory; nullptr when there is none.
+using ContourFnF = void (*)(const ContourArgsF);
+
+// The FP32 (3xTF32) alternating-layout kernel for a cubic grid; nullptr when there is none.
+ContourFnF contour_alt_kernel_f32_for(int n, int eo, size_t* smem) {
+#define CRYSSCFT_ALTF(N, E)                    \
+    {                                          \
+        *smem = AltShapeF<N, E>::SMEM;         \
+        return contour_alt_kernel_f32<N, E>;   \
+    }
+    if (eo) {
+        switch (n) {
+            case 32: CRYSSCFT_ALTF(32, true)
+            case 64: CRYSSCFT_ALTF(64, true)
+            default: break;
+        }
+    } else {
+        switch (n) {
+            case 16: CRYSSCFT_ALTF(16, false)
+            case 32: CRYSSCFT_ALTF(32, false)
+            case 48: CRYSSCFT_ALTF(48, false)
+            case 64: CRYSSCFT_ALTF(64, false)
+            default: break;
+        }
+    }
+#undef CRYSSCFT_ALTF
+    return nullptr;
+}
+
 ContourFn contour_alt_kernel_for(int n, int eo, size_t* smem) {
 #define CRYSSCFT_ALT(N, E)                     \
     {                                          \
@@ -287,9 +367,13 @@ struct scft_solver_s {
                 A = m3_axis_operator(N, (long double)cell[ax], (long double)ds_);
             CKR(upload_operator(A, (int)grid_phy[ax], *s, ax));
             pack_operator(A, (int)grid_phy[ax], *s, ax);
+            pack_operator_f32(A, (int)grid_phy[ax], *s, ax);
         }
         CKR(s->d_packed.alloc(s->h_packed.size()));
         CK(cudaMemcpy(s->d_packed.p, s->h_packed.data(), s->h_packed.size() * sizeof(double),
+                      cudaMemcpyHostToDevice));
+        CKR(s->f_packed.alloc(s->h_packed_f32.size()));
+        CK(cudaMemcpy(s->f_packed.p, s->h_packed_f32.data(), s->h_packed_f32.size() * sizeof(float),
                       cudaMemcpyHostToDevice));
         ops = s.get();
         ops_cache[ds_] = std::move(s);
@@ -356,19 +440,97 @@ struct scft_diblock_s {
     bool no_alternating = false;          // force the two-phase schedule (A/B comparisons)
     DevBuf<double> d_xch;                 // exchange buffers, 2 x space_size_phy per chain
     DevBuf<unsigned> flags;               // per-unit phase flags of the alternating kernel
+    ContourFnF contour_fn_f32 = nullptr;  // FP32 (3xTF32) contour kernel
+    DevBuf<float> f_xch;                  // FP32 exchange buffers
     DevBuf<unsigned> ctrl;                // [0] barrier arrivals, [1] error bits
     long long spin_limit = 20000000LL;
+
+    // graphs of the precision not in use (see scft_diblock_set_precision)
+    cudaGraph_t saved_graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t saved_gexec[2] = {nullptr, nullptr};
+    unsigned long long saved_gen[2] = {~0ULL, ~0ULL};
+    bool saved_use_graph[2] = {true, true};
 
     ~scft_diblock_s() {
         if (gexec) cudaGraphExecDestroy(gexec);
         if (graph) cudaGraphDestroy(graph);
+        for (int i = 0; i < 2; ++i) {
+            if (saved_gexec[i]) cudaGraphExecDestroy(saved_gexec[i]);
+            if (saved_graph[i]) cudaGraphDestroy(saved_graph[i]);
+        }
     }
 
     // Decide whether the persistent contour kernel can run this grid (FP64, every
     // axis a multiple of 8 and at most kContourMaxN, shared memory within the limit).
+    // FP32 precision form: the 3xTF32 alternating kernel for cubic grids it covers
+    int setup_persistent_f32() {
+        persistent = false;
+        const OpsSet* o = solver->ops;
+        if (!o) return SCFT_OK;
+        const int nx = (int)solver->grid_phy[0], ny = (int)solver->grid_phy[1], nz = (int)solver->grid_phy[2];
+        if (nx != ny || ny != nz || o->eo_f32[0] != o->eo_f32[1] || o->eo_f32[1] != o->eo_f32[2]) return SCFT_OK;
+        size_t smem = 0;
+        ContourFnF f = contour_alt_kernel_f32_for(nx, o->eo_f32[0], &smem);
+        if (!f) return SCFT_OK;
+        int dev_smem = 0, sms = 0;
+        CK(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, solver->device));
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, solver->device));
+        if (smem > (size_t)dev_smem) return SCFT_OK;
+        CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int per_sm = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, kContourThreads, smem));
+        if (per_sm < 1) return SCFT_OK;
+        contour_fn_f32 = f;
+        persistent_grid = std::min(2 * nx, per_sm * sms);
+        persistent_smem = smem;
+        if (!f_xch.p) CKR(f_xch.alloc(4 * M));
+        if (flags.n != (size_t)(4 * nx)) CKR(flags.alloc((size_t)4 * nx));
+        if (!ctrl.p) {
+            CKR(ctrl.alloc(2));
+            CK(cudaMemset(ctrl.p, 0, 2 * sizeof(unsigned)));
+        }
+        alternating = true;
+        persistent = true;
+        return SCFT_OK;
+    }
+
+    int launch_contour_f32(cudaStream_t st, float* wAds, float* wBds, float* q, float* qc) {
+        ContourArgsF a{};
+        a.q[0] = q;
+        a.q[1] = qc;
+        a.wds[0] = wAds;
+        a.wds[1] = wBds;
+        a.xbuf[0] = f_xch.p;
+        a.xbuf[1] = f_xch.p + 2 * M;
+        a.ops = solver->ops->f_packed.p;
+        a.nchain = 2;
+        a.slot0[0] = 0;
+        a.dir[0] = 1;
+        a.slot0[1] = (long long)U;
+        a.dir[1] = -1;
+        a.NsA = (long long)NsA;
+        a.t_end = (int)U;
+        a.error = reinterpret_cast<int*>(ctrl.p + 1);
+        a.spin_limit = spin_limit;
+        a.flags = flags.p;
+        CK(cudaMemsetAsync(flags.p, 0, flags.n * sizeof(unsigned), st));
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3((unsigned)persistent_grid);
+        cfg.blockDim = dim3(kContourThreads);
+        cfg.dynamicSmemBytes = persistent_smem;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        CK(cudaLaunchKernelEx(&cfg, contour_fn_f32, a));
+        return SCFT_OK;
+    }
+
     int setup_persistent() {
         persistent = false;
-        if (precision != SCFT_FP64) return SCFT_OK;
+        if (precision == SCFT_FP32) return setup_persistent_f32();
         const OpsSet* o = solver->ops;
         if (!o) return SCFT_OK;
         for (int ax = 0; ax < 3; ++ax) {
@@ -402,8 +564,10 @@ struct scft_diblock_s {
         const int units = 2 * (nx > ny ? nx : ny);
         persistent_grid = std::min(units, per_sm * sms);
         persistent_smem = smem;
-        if (!ctrl.p) CKR(ctrl.alloc(2));
-        CK(cudaMemset(ctrl.p, 0, 2 * sizeof(unsigned)));
+        if (!ctrl.p) {
+            CKR(ctrl.alloc(2));
+            CK(cudaMemset(ctrl.p, 0, 2 * sizeof(unsigned)));
+        }
         persistent = true;
         return SCFT_OK;
     }
@@ -464,13 +628,12 @@ struct scft_diblock_s {
         ++launches;
         if (phase_events) CK(cudaEventRecord(phase_events[1], st));
         const size_t before = solver->launches;
-        if constexpr (sizeof(T) == 8) {
-            if (persistent) {
-                CKR(launch_contour(st, wAds, wBds, q, qc));
-                ++solver->launches;
-            }
+        if (persistent) {
+            if constexpr (sizeof(T) == 8) CKR(launch_contour(st, wAds, wBds, q, qc));
+            else CKR(launch_contour_f32(st, wAds, wBds, q, qc));
+            ++solver->launches;
         }
-        for (size_t t_ = 0; t_ < U && !(persistent && sizeof(T) == 8); ++t_) {
+        for (size_t t_ = 0; t_ < U && !persistent; ++t_) {
             // forward chain: q[t] -> q[t+1] with block A (t < NsA) or B
             // backward chain: qc[U-t] -> qc[U-t-1] with the block of segment U-t-1
             const T* w1 = t_ < NsA ? wAds : wBds;
@@ -770,6 +933,55 @@ int scft_solver_propagate(scft_solver_t s, double* q, const double* init, const 
 }
 
 // ------------------------------- diblock ----------------------------------
+// Contour stores and Boltzmann factors of one precision (allocated on first use).
+static int diblock_buffers(scft_diblock_t d, int precision) {
+    const size_t M = d->M;
+    if (precision == SCFT_FP64) {
+        if (d->d_q.p) return SCFT_OK;
+        CKR(d->d_wAds.alloc(M)); CKR(d->d_wBds.alloc(M));
+        CKR(d->d_q.alloc((d->U + 1) * M)); CKR(d->d_qc.alloc((d->U + 1) * M));
+        for (int i = 0; i < 4; ++i) CKR(d->d_t[i].alloc(M));
+    } else {
+        if (d->f_q.p) return SCFT_OK;
+        CKR(d->f_wAds.alloc(M)); CKR(d->f_wBds.alloc(M));
+        CKR(d->f_q.alloc((d->U + 1) * M)); CKR(d->f_qc.alloc((d->U + 1) * M));
+        for (int i = 0; i < 4; ++i) CKR(d->f_t[i].alloc(M));
+    }
+    return SCFT_OK;
+}
+
+int scft_diblock_set_precision(scft_diblock_t d, int precision) {
+    if (!d) return fail(SCFT_ERR_INVALID_ARG, "null handle");
+    if (precision != SCFT_FP64 && precision != SCFT_FP32) return fail(SCFT_ERR_INVALID_ARG, "bad precision");
+    if (precision == d->precision) return SCFT_OK;
+    CK(cudaSetDevice(d->solver->device));
+    CK(cudaStreamSynchronize(d->solver->stream));
+    CKR(diblock_buffers(d, precision));
+    // keep the captured graph of each precision: switching back and forth (FP32 iterations,
+    // then FP64 polish) replays instead of re-capturing
+    const int o = d->precision, n = precision;
+    d->saved_graph[o] = d->graph;
+    d->saved_gexec[o] = d->gexec;
+    d->saved_gen[o] = d->captured_gen;
+    d->saved_use_graph[o] = d->use_graph;
+    d->graph = d->saved_graph[n];
+    d->gexec = d->saved_gexec[n];
+    d->captured_gen = d->saved_gen[n];
+    d->use_graph = d->saved_use_graph[n];
+    d->saved_graph[n] = nullptr;
+    d->saved_gexec[n] = nullptr;
+    d->precision = n;
+    // the persistent-kernel plan of this precision (host-side choices only)
+    if (d->solver->ops && d->captured_gen == d->solver->ops_gen) CKR(d->setup_persistent());
+    return SCFT_OK;
+}
+
+int scft_diblock_get_precision(scft_diblock_t d, int* out) {
+    if (!d || !out) return fail(SCFT_ERR_INVALID_ARG, "null argument");
+    *out = d->precision;
+    return SCFT_OK;
+}
+
 int scft_diblock_create(scft_solver_t s, double fA, double ds, double xN, double acceptance,
                         scft_diblock_t* out) {
     if (!s || !out) return fail(SCFT_ERR_INVALID_ARG, "null argument");
@@ -797,15 +1009,7 @@ int scft_diblock_create(scft_solver_t s, double fA, double ds, double xN, double
     CK(cudaMemset(d->state.p, 0, sizeof(IterState)));
     CK(cudaMemset(d->phiA.p, 0, M * sizeof(double)));
     CK(cudaMemset(d->phiB.p, 0, M * sizeof(double)));
-    if (d->precision == SCFT_FP64) {
-        CKR(d->d_wAds.alloc(M)); CKR(d->d_wBds.alloc(M));
-        CKR(d->d_q.alloc((d->U + 1) * M)); CKR(d->d_qc.alloc((d->U + 1) * M));
-        for (int i = 0; i < 4; ++i) CKR(d->d_t[i].alloc(M));
-    } else {
-        CKR(d->f_wAds.alloc(M)); CKR(d->f_wBds.alloc(M));
-        CKR(d->f_q.alloc((d->U + 1) * M)); CKR(d->f_qc.alloc((d->U + 1) * M));
-        for (int i = 0; i < 4; ++i) CKR(d->f_t[i].alloc(M));
-    }
+    CKR(diblock_buffers(d.get(), d->precision));
     *out = d.release();
     return SCFT_OK;
 }

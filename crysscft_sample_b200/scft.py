@@ -113,6 +113,25 @@ class DiblockSCFT:
         check(_lib.load().scft_diblock_device_fields(self._h, *[ctypes.byref(p) for p in ps]))
         return tuple(p.value for p in ps)
 
+    def set_precision(self, precision: str):
+        """"fp64" (plain form) or "fp32" (3xTF32 triplets, FP64 Q/phi/energy/mixing)."""
+        check(_lib.load().scft_diblock_set_precision(self._h, _lib.PRECISION[precision]))
+
+    def get_precision(self) -> str:
+        v = ctypes.c_int()
+        check(_lib.load().scft_diblock_get_precision(self._h, ctypes.byref(v)))
+        return {0: "fp64", 1: "fp32"}[v.value]
+
+    def iterate_polished(self, n_iter: int, n_polish: int):
+        """The precision form: n_iter - n_polish FP32 iterations, then n_polish FP64 ones."""
+        self.set_precision("fp32")
+        h1 = self.iterate(n_iter - n_polish) if n_iter > n_polish else None
+        self.set_precision("fp64")
+        h2 = self.iterate(n_polish)
+        if h1 is None:
+            return h2
+        return {k: np.concatenate([h1[k], h2[k]]) for k in h2}
+
     def time_phases(self, n_iter: int):
         """ms per iteration: (total, propagator chains, Q + phi, the rest); advances the fields."""
         out = np.zeros(4)

@@ -139,6 +139,14 @@ int scft_diblock_iterate_host(scft_diblock_t d, double* wA, double* wB, size_t n
                               double* phiA, double* phiB, double* F, double* parts,
                               double* maxinc, double* Q);
 
+/* Arithmetic of the contour chains for the following iterations: SCFT_FP64 (the plain
+ * form) or SCFT_FP32 (FP32 triplets on the tensor cores as 3xTF32 split products; Q,
+ * phi, the free energy and the mixing stay FP64).  The precision form runs most
+ * iterations in FP32 and finishes with FP64 "polish" iterations.  No counterpart in
+ * the reference (FP64 only).  Buffers of a precision are allocated on first use. */
+int scft_diblock_set_precision(scft_diblock_t d, int precision);
+int scft_diblock_get_precision(scft_diblock_t d, int* out);
+
 /* Number of kernel launches the last scft_diblock_iterate issued per iteration. */
 int scft_diblock_launches_per_iteration(scft_diblock_t d, size_t* out);
 
