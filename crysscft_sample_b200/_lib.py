@@ -55,6 +55,7 @@ SIGNATURES = {
     "scft_solver_diffusion_device_static_scratch": (ctypes.c_int, [_vp, _vp, _vp]),
     "scft_measure_fp64_peak": (ctypes.c_int, [ctypes.c_int, _dp, _dp]),
     "scft_diblock_set_precision": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "scft_diblock_get_contour": (ctypes.c_int, [_vp, ctypes.c_int, _sz, _dp]),
     "scft_diblock_get_precision": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int)]),
 }
 

@@ -1053,6 +1053,27 @@ int scft_diblock_get_fields(scft_diblock_t d, double* phiA, double* phiB, double
     return SCFT_OK;
 }
 
+int scft_diblock_get_contour(scft_diblock_t d, int chain, size_t slot, double* out) {
+    if (!d || !out) return fail(SCFT_ERR_INVALID_ARG, "null argument");
+    if (chain != 0 && chain != 1) return fail(SCFT_ERR_INVALID_ARG, "chain must be 0 (q) or 1 (q+)");
+    if (slot > d->U) return fail(SCFT_ERR_INVALID_ARG, "slot beyond NsA + NsB");
+    CK(cudaSetDevice(d->solver->device));
+    cudaStream_t st = d->solver->stream;
+    const size_t M = d->M;
+    if (d->precision == SCFT_FP64) {
+        const double* src = (chain ? d->d_qc.p : d->d_q.p) + slot * M;
+        CK(cudaMemcpyAsync(out, src, M * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+    } else {
+        std::vector<float> tmp(M);
+        const float* src = (chain ? d->f_qc.p : d->f_q.p) + slot * M;
+        CK(cudaMemcpyAsync(tmp.data(), src, M * sizeof(float), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        for (size_t i = 0; i < M; ++i) out[i] = tmp[i];
+    }
+    return SCFT_OK;
+}
+
 int scft_diblock_device_fields(scft_diblock_t d, double** phiA, double** phiB, double** wA, double** wB) {
     if (!d) return fail(SCFT_ERR_INVALID_ARG, "null handle");
     if (phiA) *phiA = d->phiA.p;

@@ -113,6 +113,12 @@ class DiblockSCFT:
         check(_lib.load().scft_diblock_device_fields(self._h, *[ctypes.byref(p) for p in ps]))
         return tuple(p.value for p in ps)
 
+    def get_contour(self, chain: int, slot: int) -> np.ndarray:
+        """Stored propagator slice of the last iteration (chain 0: q, chain 1: q+)."""
+        out = np.empty(self.M)
+        check(_lib.load().scft_diblock_get_contour(self._h, int(chain), int(slot), _lib.dptr(out)))
+        return out
+
     def set_precision(self, precision: str):
         """"fp64" (plain form) or "fp32" (3xTF32 triplets, FP64 Q/phi/energy/mixing)."""
         check(_lib.load().scft_diblock_set_precision(self._h, _lib.PRECISION[precision]))

@@ -122,6 +122,12 @@ int scft_diblock_get_contour_counts(scft_diblock_t d, size_t* NsA, size_t* NsB);
 int scft_diblock_set_fields(scft_diblock_t d, const double* wA, const double* wB);
 /* Copy phiA, phiB (of the last iteration) and wA, wB (after its update) to host; any may be NULL. */
 int scft_diblock_get_fields(scft_diblock_t d, double* phiA, double* phiB, double* wA, double* wB);
+/* Copy one stored propagator slice of the last iteration to host (as FP64): chain 0 is
+ * q (slot u: qA(u) for u <= NsA, qB(u-NsA) after), chain 1 is q+ (qcA(u), then
+ * qcB(u-NsA)); slot in [0, NsA+NsB].  The reference's qA/qB/qcA/qcB arrays
+ * (src/crysSCFT_sample.cpp:457-460) hold the same values. */
+int scft_diblock_get_contour(scft_diblock_t d, int chain, size_t slot, double* out);
+
 /* Device pointers of the resident fields (space_size_phy FP64 each); any out may be NULL. */
 int scft_diblock_device_fields(scft_diblock_t d, double** phiA, double** phiB, double** wA,
                                double** wB);
