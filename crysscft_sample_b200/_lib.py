@@ -56,6 +56,7 @@ SIGNATURES = {
     "scft_measure_fp64_peak": (ctypes.c_int, [ctypes.c_int, _dp, _dp]),
     "scft_diblock_set_precision": (ctypes.c_int, [_vp, ctypes.c_int]),
     "scft_diblock_get_contour": (ctypes.c_int, [_vp, ctypes.c_int, _sz, _dp]),
+    "scft_diblock_stress": (ctypes.c_int, [_vp, _dp, _dp, _dp]),
     "scft_diblock_get_precision": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int)]),
 }
 

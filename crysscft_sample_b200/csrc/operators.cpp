@@ -93,3 +93,69 @@ std::vector<long double> m3_axis_operator(int N, long double L, long double ds) 
 }
 
 }  // namespace crysscft
+
+// ---------------------------------------------------------------------------
+// Cell-length derivatives.  Every operator above is linear in its spectral factor
+// g_k = exp(-ds (2 pi k / L)^2), and dg_k/dL = g_k * 2 ds (2 pi k)^2 / L^3, so the
+// derivative operator is the same construction with g replaced by dg/dL.
+// ---------------------------------------------------------------------------
+namespace crysscft {
+
+static long double dgauss_dL(long k, long double L, long double ds) {
+    const long double kk = 2.0L * kPi * (long double)k;
+    return gauss(k, L, ds) * 2.0L * ds * kk * kk / (L * L * L);
+}
+
+std::vector<long double> pmmm_axis_operator_dL(int n, long double L, long double ds) {
+    const long period = 4L * n;
+    std::vector<long double> ctab(period);
+    for (long m = 0; m < period; ++m) ctab[m] = cosl(kPi * (long double)m / (2.0L * n));
+    std::vector<long double> g(n);
+    for (int k = 0; k < n; ++k) g[k] = dgauss_dL(k, L, ds) * (k == 0 ? 1.0L : 2.0L);
+    std::vector<long double> A((size_t)n * n);
+    for (int j = 0; j < n; ++j)
+        for (int jp = 0; jp < n; ++jp) {
+            long double acc = 0.0L;
+            for (int k = 0; k < n; ++k)
+                acc += g[k] * ctab[((long)k * (2 * j + 1)) % period] * ctab[((long)k * (2 * jp + 1)) % period];
+            A[(size_t)j * n + jp] = acc / (long double)n;
+        }
+    return A;
+}
+
+static std::vector<long double> circulant_kernel_dL(int N, long double L, long double ds) {
+    std::vector<long double> ctab(N);
+    for (int m = 0; m < N; ++m) ctab[m] = cosl(2.0L * kPi * (long double)m / (long double)N);
+    std::vector<long double> g(N);
+    for (int k = 0; k < N; ++k) g[k] = dgauss_dL(k < N - k ? k : N - k, L, ds);
+    std::vector<long double> c(N);
+    for (int d = 0; d < N; ++d) {
+        long double acc = 0.0L;
+        for (int k = 0; k < N; ++k) acc += g[k] * ctab[((long)k * d) % N];
+        c[d] = acc / (long double)N;
+    }
+    return c;
+}
+
+std::vector<long double> p1_axis_operator_dL(int N, long double L, long double ds) {
+    std::vector<long double> c = circulant_kernel_dL(N, L, ds);
+    std::vector<long double> A((size_t)N * N);
+    for (int i = 0; i < N; ++i)
+        for (int j = 0; j < N; ++j) A[(size_t)i * N + j] = c[((i - j) % N + N) % N];
+    return A;
+}
+
+std::vector<long double> m3_axis_operator_dL(int N, long double L, long double ds) {
+    const int n = N / 2;
+    std::vector<long double> c = circulant_kernel_dL(N, L, ds);
+    std::vector<long double> A((size_t)n * n);
+    for (int i = 0; i < n; ++i)
+        for (int ip = 0; ip < n; ++ip) {
+            long d1 = ((2L * i - 2L * ip) % N + N) % N;
+            long d2 = ((2L * i + 2L * ip + 1 - N) % N + N) % N;
+            A[(size_t)i * n + ip] = c[d1] + c[d2];
+        }
+    return A;
+}
+
+}  // namespace crysscft

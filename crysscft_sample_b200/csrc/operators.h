@@ -13,4 +13,9 @@ std::vector<long double> p1_axis_operator(int N, long double L, long double ds);
 // CrysPSSolver3m (zero translations), one axis of n = N/2 even-sub-lattice points
 std::vector<long double> m3_axis_operator(int N, long double L, long double ds);
 
+// d/dL of the same operators (the cell-length derivative used by the stress)
+std::vector<long double> pmmm_axis_operator_dL(int n, long double L, long double ds);
+std::vector<long double> p1_axis_operator_dL(int N, long double L, long double ds);
+std::vector<long double> m3_axis_operator_dL(int N, long double L, long double ds);
+
 }  // namespace crysscft

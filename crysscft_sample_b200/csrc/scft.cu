@@ -21,6 +21,7 @@
 #include "contour_kernel_f32.cuh"
 #include "field_kernels.cuh"
 #include "operators.h"
+#include "stress_kernels.cuh"
 
 using namespace crysscft;
 
@@ -87,6 +88,9 @@ struct OpsSet {
     std::vector<float> h_packed_f32;
     DevBuf<float> f_packed;
     int eo_f32[3] = {0, 0, 0};
+    // cell-length derivatives dA/dL of the three axis operators (built on first use)
+    DevBuf<double> d_dop[3], d_dopT[3];
+    bool have_dop = false;
 };
 
 // Round an FP32 value to the TF32 format (10 explicit mantissa bits), to nearest with
@@ -381,6 +385,52 @@ struct scft_solver_s {
         return SCFT_OK;
     }
 
+    // the cell-length derivative operators of the current (cell, ds)
+    int build_dops() {
+        if (!ops) return fail(SCFT_ERR_NOT_READY, "set_cell_para/set_contour_step first");
+        if (ops->have_dop) return SCFT_OK;
+        for (int ax = 0; ax < 3; ++ax) {
+            const int N = (int)grid_log[ax];
+            const int n = (int)grid_phy[ax];
+            std::vector<long double> A;
+            if (kind == SCFT_SOLVER_PMMM)
+                A = pmmm_axis_operator_dL(N / 2, (long double)cell[0], (long double)ds);
+            else if (kind == SCFT_SOLVER_P1)
+                A = p1_axis_operator_dL(N, (long double)cell[ax], (long double)ds);
+            else
+                A = m3_axis_operator_dL(N, (long double)cell[ax], (long double)ds);
+            std::vector<double> d((size_t)n * n), dt((size_t)n * n);
+            for (int i = 0; i < n; ++i)
+                for (int j = 0; j < n; ++j) {
+                    d[(size_t)i * n + j] = (double)A[(size_t)i * n + j];
+                    dt[(size_t)j * n + i] = (double)A[(size_t)i * n + j];
+                }
+            CKR(ops->d_dop[ax].alloc((size_t)n * n));
+            CKR(ops->d_dopT[ax].alloc((size_t)n * n));
+            CK(cudaMemcpy(ops->d_dop[ax].p, d.data(), d.size() * sizeof(double), cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(ops->d_dopT[ax].p, dt.data(), dt.size() * sizeof(double), cudaMemcpyHostToDevice));
+        }
+        ops->have_dop = true;
+        return SCFT_OK;
+    }
+
+    // (op_x (x) op_y (x) op_z) applied to nt stacked fields: in -> t1 -> t2 -> out
+    int triplet_batched(const double* in, double* out, double* t1, double* t2, long long nt,
+                        const double* const op[3], const double* const opT[3], cudaStream_t st) {
+        const int nx = (int)grid_phy[0], ny = (int)grid_phy[1], nz = (int)grid_phy[2];
+        AxisPass<double> pz{}, py{}, px{};
+        pz.ch[0] = ChainIO<double>{in, t1, nullptr, nullptr};
+        py.ch[0] = ChainIO<double>{t1, t2, nullptr, nullptr};
+        px.ch[0] = ChainIO<double>{t2, out, nullptr, nullptr};
+        pz.op = op[2]; pz.opT = opT[2]; pz.n = nz; pz.outer = nt * nx * ny; pz.inner = 1;
+        py.op = op[1]; py.opT = opT[1]; py.n = ny; py.outer = nt * nx; py.inner = nz;
+        px.op = op[0]; px.opT = opT[0]; px.n = nx; px.outer = nt; px.inner = (long long)ny * nz;
+        CK(launch_axis(pz, 1, true, st));
+        CK(launch_axis(py, 1, false, st));
+        CK(launch_axis(px, 1, false, st));
+        return SCFT_OK;
+    }
+
     // one triplet per chain: in -> (pre) z-pass -> t1 -> y-pass -> t2 -> x-pass (post) -> out
     template <typename T>
     int triplet(int nchain, const ChainIO<T> io[2], T* t1[2], T* t2[2], cudaStream_t st) {
@@ -440,6 +490,8 @@ struct scft_diblock_s {
     bool no_alternating = false;          // force the two-phase schedule (A/B comparisons)
     DevBuf<double> d_xch;                 // exchange buffers, 2 x space_size_phy per chain
     DevBuf<unsigned> flags;               // per-unit phase flags of the alternating kernel
+    int last_iter_precision = -1;         // precision of the iteration whose contour is stored
+    DevBuf<double> stress_buf;            // batched temporaries of scft_diblock_stress
     ContourFnF contour_fn_f32 = nullptr;  // FP32 (3xTF32) contour kernel
     DevBuf<float> f_xch;                  // FP32 exchange buffers
     DevBuf<unsigned> ctrl;                // [0] barrier arrivals, [1] error bits
@@ -1053,6 +1105,79 @@ int scft_diblock_get_fields(scft_diblock_t d, double* phiA, double* phiB, double
     return SCFT_OK;
 }
 
+int scft_diblock_stress(scft_diblock_t d, double dlnQ_dL[3], double* dF_dxN, double* Q_out) {
+    if (!d) return fail(SCFT_ERR_INVALID_ARG, "null handle");
+    if (d->last_iter_precision != SCFT_FP64)
+        return fail(SCFT_ERR_NOT_READY, "the stress needs the stored contour of an FP64 iteration");
+    scft_solver_t s = d->solver;
+    CK(cudaSetDevice(s->device));
+    if (!s->ds_set || !s->ops || s->ds != d->ds) CKR(scft_solver_set_contour_step(s, d->ds));
+    CKR(s->build_dops());
+    cudaStream_t st = s->stream;
+    const long long M = (long long)d->M;
+    const long long U = (long long)d->U, NsA = (long long)d->NsA;
+    IterState hs{};
+    CK(cudaMemcpyAsync(&hs, d->state.p, sizeof(IterState), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    const double Q = hs.Q;
+    if (!(Q > 0.0)) return fail(SCFT_ERR_NOT_READY, "no iteration has run");
+    // slices per batch: about 64 MB per temporary field array
+    long long tc = (64LL << 20) / (M * (long long)sizeof(double));
+    if (tc < 1) tc = 1;
+    if (tc > U) tc = U;
+    if (d->stress_buf.n < (size_t)(4 * tc * M)) CKR(d->stress_buf.alloc((size_t)(4 * tc * M)));
+    double* X = d->stress_buf.p;
+    double* Y = X + tc * M;
+    double* T1 = Y + tc * M;
+    double* T2 = T1 + tc * M;
+    const int rblocks = (int)std::min<long long>(kRedMaxBlocks, (tc * M + kRedThreads - 1) / kRedThreads);
+    std::vector<double> part(kRedMaxBlocks);
+    for (int ax = 0; ax < 3; ++ax) {
+        const double* op[3];
+        const double* opT[3];
+        for (int b = 0; b < 3; ++b) {
+            op[b] = b == ax ? s->ops->d_dop[b].p : s->ops->d_op[b].p;
+            opT[b] = b == ax ? s->ops->d_dopT[b].p : s->ops->d_opT[b].p;
+        }
+        double acc = 0.0;
+        for (int blk = 0; blk < 2; ++blk) {
+            const long long lo = blk == 0 ? 0 : NsA, hi = blk == 0 ? NsA : U;
+            const double* D = blk == 0 ? d->d_wAds.p : d->d_wBds.p;
+            for (long long t0 = lo; t0 < hi; t0 += tc) {
+                const long long nt = std::min(tc, hi - t0);
+                stress_scale_kernel<<<grid_blocks(nt * M, 256), 256, 0, st>>>(X, d->d_q.p, D, t0, nt, M);
+                CK(cudaGetLastError());
+                CKR(s->triplet_batched(X, Y, T1, T2, nt, op, opT, st));
+                const int nb = (int)std::min<long long>(rblocks, (nt * M + kRedThreads - 1) / kRedThreads);
+                stress_dot_kernel<<<nb, kRedThreads, 0, st>>>(d->d_qc.p, D, Y, t0, nt, M, d->partials.p);
+                CK(cudaGetLastError());
+                CK(cudaMemcpyAsync(part.data(), d->partials.p, nb * sizeof(double), cudaMemcpyDeviceToHost, st));
+                CK(cudaStreamSynchronize(st));
+                for (int i = 0; i < nb; ++i) acc += part[i];
+            }
+        }
+        if (dlnQ_dL) dlnQ_dL[ax] = acc / (double)M / Q;
+    }
+    if (dF_dxN) {
+        // F (src/crysSCFT_sample.cpp:404-418) at fixed fields: d(xN <phiA phiB>)/dxN = <phiA phiB>,
+        // and ksi = (wA + wB - xN)/2 gives d<-ksi (1 - phiA - phiB)>/dxN = <1 - phiA - phiB>/2
+        const int nb = (int)std::min<long long>(kRedMaxBlocks, (M + kRedThreads - 1) / kRedThreads);
+        dxn_terms_kernel<<<nb, kRedThreads, 0, st>>>(d->phiA.p, d->phiB.p, M, d->partials.p);
+        CK(cudaGetLastError());
+        std::vector<double> p2(2 * nb);
+        CK(cudaMemcpyAsync(p2.data(), d->partials.p, p2.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        double ab = 0.0, inc = 0.0;
+        for (int i = 0; i < nb; ++i) {
+            ab += p2[2 * i];
+            inc += p2[2 * i + 1];
+        }
+        *dF_dxN = ab / (double)M + 0.5 * inc / (double)M;
+    }
+    if (Q_out) *Q_out = Q;
+    return SCFT_OK;
+}
+
 int scft_diblock_get_contour(scft_diblock_t d, int chain, size_t slot, double* out) {
     if (!d || !out) return fail(SCFT_ERR_INVALID_ARG, "null argument");
     if (chain != 0 && chain != 1) return fail(SCFT_ERR_INVALID_ARG, "chain must be 0 (q) or 1 (q+)");
@@ -1129,6 +1254,7 @@ static int diblock_run(scft_diblock_t d, size_t n_iter, double* F, double* parts
         CK(cudaMemcpyAsync(h.data(), d->hist.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         CKR(diblock_check_device_error(d, st));
+        if (chunk) d->last_iter_precision = d->precision;
         bool bad = false;
         for (size_t i = 0; i < chunk; ++i) {
             const double* r = &h[i * HIST_STRIDE];
@@ -1203,6 +1329,7 @@ int scft_diblock_time_phases(scft_diblock_t d, size_t n_iter, double out[4]) {
     d->phase_events = nullptr;
     for (auto& e : ev) cudaEventDestroy(e);
     for (int i = 0; i < 4; ++i) out[i] = n_iter ? acc[i] / (double)n_iter : 0.0;
+    if (n_iter) d->last_iter_precision = d->precision;
     return diblock_check_device_error(d, st);
 }
 

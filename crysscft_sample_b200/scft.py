@@ -113,6 +113,14 @@ class DiblockSCFT:
         check(_lib.load().scft_diblock_device_fields(self._h, *[ctypes.byref(p) for p in ps]))
         return tuple(p.value for p in ps)
 
+    def stress(self):
+        """Backward pass from the last FP64 iteration: d ln Q / d L (3 axes), dF/dchiN, Q.
+        At the saddle point the stress is dF/dL = -dlnQ_dL."""
+        g = np.zeros(3)
+        dx, Q = ctypes.c_double(), ctypes.c_double()
+        check(_lib.load().scft_diblock_stress(self._h, _lib.dptr(g), ctypes.byref(dx), ctypes.byref(Q)))
+        return {"dlnQ_dL": g, "dF_dxN": dx.value, "Q": Q.value}
+
     def get_contour(self, chain: int, slot: int) -> np.ndarray:
         """Stored propagator slice of the last iteration (chain 0: q, chain 1: q+)."""
         out = np.empty(self.M)
@@ -148,6 +156,43 @@ class DiblockSCFT:
         v = ctypes.c_size_t()
         check(_lib.load().scft_diblock_launches_per_iteration(self._h, ctypes.byref(v)))
         return v.value
+
+
+def relax_cell(solver, fA, ds, xN, acceptance, wA, wB, L0, n_outer=40, n_inner=20, step=1.0, tol=1e-6,
+               cubic=True):
+    """Variable-cell relaxation: n_inner SCFT iterations at the current cell, then a
+    gradient step L <- L - step * dF/dL with the saddle-point stress dF/dL = -dlnQ/dL
+    (cubic: one length, the sum over axes).  Stops when |dF/dL| < tol.  Returns the
+    history of (L, F, dF/dL) and the final fields."""
+    L = np.array(L0 if np.ndim(L0) else (L0, L0, L0), dtype=np.float64)
+    run = None
+    hist = []
+    w = (np.asarray(wA, dtype=np.float64).ravel().copy(), np.asarray(wB, dtype=np.float64).ravel().copy())
+    for _ in range(n_outer):
+        solver.set_cell_para(tuple(L))
+        if run is None:
+            run = DiblockSCFT(solver, fA, ds, xN, acceptance)
+        run.set_fields(*w)
+        h = run.iterate(n_inner)
+        s = run.stress()
+        f = run.get_fields()
+        w = (f["wA"], f["wB"])
+        g = -s["dlnQ_dL"]
+        if cubic:
+            gc = float(g.sum())
+            hist.append((float(L[0]), float(h["F"][-1]), gc))
+            if abs(gc) < tol:
+                break
+            L = L - step * gc
+        else:
+            hist.append((L.copy(), float(h["F"][-1]), g.copy()))
+            if np.abs(g).max() < tol:
+                break
+            L = L - step * g
+    out = {"history": hist, "L": L}
+    out.update(run.get_fields())
+    run.close()
+    return out
 
 
 def diblock_scft_simple_iterate(Nx, Ny, Nz, fA, ds, xN, Lx, Ly, Lz, acceptance, Nstep, solvername, solver,

@@ -122,6 +122,18 @@ int scft_diblock_get_contour_counts(scft_diblock_t d, size_t* NsA, size_t* NsB);
 int scft_diblock_set_fields(scft_diblock_t d, const double* wA, const double* wB);
 /* Copy phiA, phiB (of the last iteration) and wA, wB (after its update) to host; any may be NULL. */
 int scft_diblock_get_fields(scft_diblock_t d, double* phiA, double* phiB, double* wA, double* wB);
+/* Backward pass of the differentiation form, from the stored contour of the last (FP64)
+ * iteration: dlnQ_dL[a] = d ln Q / d L_a at fixed fields, by the adjoint identity
+ * dQ/dL_a = (1/M) sum_t < q+[t+1], D_t (dT/dL_a) D_t q[t] > (one term per contour step;
+ * T = A_x (x) A_y (x) A_z, so dT/dL_x = (dA_x/dL_x) (x) A_y (x) A_z).  The stress
+ * dF/dL_a equals -dlnQ_dL[a] at the SCFT saddle point (there dF/dphi = 0).  For PMMM
+ * (cubic cell in the reference) the three axis derivatives are still reported; the
+ * cubic dF/dL is minus their sum.  dF_dxN = dF/dchiN at fixed fields, from the energy
+ * terms of print_energy (src/crysSCFT_sample.cpp:404-418): <phiA phiB> +
+ * <1 - phiA - phiB>/2.  Q_out: the Q of that iteration.  Any output may be NULL.
+ * No counterpart in the reference (it has no derivatives). */
+int scft_diblock_stress(scft_diblock_t d, double dlnQ_dL[3], double* dF_dxN, double* Q_out);
+
 /* Copy one stored propagator slice of the last iteration to host (as FP64): chain 0 is
  * q (slot u: qA(u) for u <= NsA, qB(u-NsA) after), chain 1 is q+ (qcA(u), then
  * qcB(u-NsA)); slot in [0, NsA+NsB].  The reference's qA/qB/qcA/qcB arrays
