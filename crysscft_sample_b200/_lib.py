@@ -57,6 +57,16 @@ SIGNATURES = {
     "scft_diblock_set_precision": (ctypes.c_int, [_vp, ctypes.c_int]),
     "scft_diblock_get_contour": (ctypes.c_int, [_vp, ctypes.c_int, _sz, _dp]),
     "scft_diblock_stress": (ctypes.c_int, [_vp, _dp, _dp, _dp]),
+    "scft_batch_create": (ctypes.c_int, [ctypes.c_int, _sz, _szp, _dp, _dp, _dp, ctypes.c_double, ctypes.c_double,
+                                         ctypes.c_int, ctypes.c_int, ctypes.POINTER(_vp)]),
+    "scft_batch_destroy": (ctypes.c_int, [_vp]),
+    "scft_batch_size": (ctypes.c_int, [_vp, _szp]),
+    "scft_batch_instance": (ctypes.c_int, [_vp, _sz, ctypes.POINTER(_vp)]),
+    "scft_batch_set_fields": (ctypes.c_int, [_vp, _sz, _dp, _dp]),
+    "scft_batch_get_fields": (ctypes.c_int, [_vp, _sz, _dp, _dp, _dp, _dp]),
+    "scft_batch_iterate": (ctypes.c_int, [_vp, _sz, _dp, _dp]),
+    "scft_batch_configure": (ctypes.c_int, [_vp, _sz, ctypes.c_int]),
+    "scft_batch_autotune": (ctypes.c_int, [_vp, _sz, _szp, ctypes.POINTER(ctypes.c_int), _dp]),
     "scft_diblock_get_precision": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int)]),
 }
 

@@ -1,0 +1,100 @@
+"""Batching form: many independent AB-diblock SCFT instances advanced together on one
+GPU (scft_batch_* in include/crysscft_b200.h).  One batch iteration is one CUDA-graph
+launch in which the instances' contour kernels run concurrently; an autotuner picks
+the number of worker streams and the contour-kernel form."""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib, fields
+from ._lib import check
+
+__all__ = ["BatchSCFT", "batch_config", "FORMS"]
+
+FORMS = {0: "automatic", 1: "alternating layout", 2: "two-phase", 3: "per-axis kernels"}
+
+
+def batch_config(n: int = 64, seed: int = 20261203, sizes=(16, 24, 32, 48, 64)):
+    """The seeded batching workload: n PMMM instances with reduced grids drawn from
+    `sizes`^3 (full grids twice that), chiN ~ U[14, 30], fA ~ U[0.2, 0.35],
+    L ~ U[3.8, 5.5] Rg, BCC or FCC seed fields."""
+    u = fields.uniform53(seed, 99, 5 * n).reshape(n, 5)
+    out = []
+    for i in range(n):
+        nr = sizes[min(int(u[i, 0] * len(sizes)), len(sizes) - 1)]
+        out.append({
+            "N": (2 * nr,) * 3,
+            "xN": 14.0 + 16.0 * u[i, 1],
+            "fA": 0.2 + 0.15 * u[i, 2],
+            "L": 3.8 + 1.7 * u[i, 3],
+            "phase": "BCC" if u[i, 4] < 0.5 else "FCC",
+            "seed": seed + 1000 + i,
+        })
+    return out
+
+
+class BatchSCFT:
+    """n instances of one solver kind; per-instance grid, cell, fA and chiN."""
+
+    def __init__(self, kind: str, instances, ds: float = 0.01, acceptance: float = 0.1,
+                 precision: str = "fp64", device: int = -1):
+        L = _lib.load()
+        n = len(instances)
+        grid = (ctypes.c_size_t * (3 * n))(*[int(v) for it in instances for v in it["N"]])
+        cell = np.array([[it["L"]] * 3 if np.ndim(it["L"]) == 0 else list(it["L"]) for it in instances],
+                        dtype=np.float64).ravel()
+        fA = np.array([it["fA"] for it in instances], dtype=np.float64)
+        xN = np.array([it["xN"] for it in instances], dtype=np.float64)
+        h = ctypes.c_void_p()
+        check(L.scft_batch_create(_lib.KIND[kind.upper()], n, grid, _lib.dptr(cell), _lib.dptr(fA), _lib.dptr(xN),
+                                  float(ds), float(acceptance), _lib.PRECISION[precision], int(device),
+                                  ctypes.byref(h)))
+        self._h = h
+        self.kind = kind.upper()
+        self.instances = instances
+        self.n = n
+        self.M = [int(np.prod([v // (1 if self.kind == "P1" else 2) for v in it["N"]])) for it in instances]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().scft_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def seed_fields(self):
+        """Seeded BCC/FCC fields of every instance (layout of the solver kind)."""
+        for i, it in enumerate(self.instances):
+            wA, wB = fields.seed_fields(it["N"], it["L"], it.get("phase", "BCC"), seed=it.get("seed", 20261203))
+            self.set_fields(i, fields.to_physical(self.kind, wA), fields.to_physical(self.kind, wB))
+
+    def set_fields(self, i: int, wA, wB):
+        wA = np.ascontiguousarray(wA, dtype=np.float64).ravel()
+        wB = np.ascontiguousarray(wB, dtype=np.float64).ravel()
+        check(_lib.load().scft_batch_set_fields(self._h, int(i), _lib.dptr(wA), _lib.dptr(wB)))
+
+    def get_fields(self, i: int):
+        out = [np.empty(self.M[i]) for _ in range(4)]
+        check(_lib.load().scft_batch_get_fields(self._h, int(i), *[_lib.dptr(a) for a in out]))
+        return dict(zip(("phiA", "phiB", "wA", "wB"), out))
+
+    def iterate(self, n_iter: int):
+        F = np.empty((n_iter, self.n))
+        mi = np.empty((n_iter, self.n))
+        check(_lib.load().scft_batch_iterate(self._h, int(n_iter), _lib.dptr(F), _lib.dptr(mi)))
+        return {"F": F, "maxinc": mi}
+
+    def configure(self, nstreams: int, form: int = 0):
+        check(_lib.load().scft_batch_configure(self._h, int(nstreams), int(form)))
+
+    def autotune(self, n_trial: int = 3):
+        ns, form, ms = ctypes.c_size_t(), ctypes.c_int(), ctypes.c_double()
+        check(_lib.load().scft_batch_autotune(self._h, int(n_trial), ctypes.byref(ns), ctypes.byref(form),
+                                              ctypes.byref(ms)))
+        return {"nstreams": ns.value, "form": FORMS[form.value], "ms_per_iteration": ms.value}

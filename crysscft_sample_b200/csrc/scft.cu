@@ -487,7 +487,8 @@ struct scft_diblock_s {
     size_t persistent_smem = 0;
     ContourFn contour_fn = nullptr;
     bool alternating = false;             // contour_fn is the alternating-layout kernel
-    bool no_alternating = false;          // force the two-phase schedule (A/B comparisons)
+    int force_form = 0;                   // 0 auto, 1 alternating, 2 two-phase, 3 per-axis kernels
+    int last_form = 0;                    // force_form the current launch plan was built with
     DevBuf<double> d_xch;                 // exchange buffers, 2 x space_size_phy per chain
     DevBuf<unsigned> flags;               // per-unit phase flags of the alternating kernel
     int last_iter_precision = -1;         // precision of the iteration whose contour is stored
@@ -582,6 +583,8 @@ struct scft_diblock_s {
 
     int setup_persistent() {
         persistent = false;
+        alternating = false;
+        if (force_form == 3) return SCFT_OK;  // per-axis kernels only
         if (precision == SCFT_FP32) return setup_persistent_f32();
         const OpsSet* o = solver->ops;
         if (!o) return SCFT_OK;
@@ -598,7 +601,7 @@ struct scft_diblock_s {
         if (smem > (size_t)dev_smem) return SCFT_OK;
         contour_fn = contour_kernel_for(nx, ny, nz, o->eo);
         alternating = false;
-        if (nx == ny && ny == nz && o->eo[0] == o->eo[1] && o->eo[1] == o->eo[2] && !no_alternating) {
+        if (nx == ny && ny == nz && o->eo[0] == o->eo[1] && o->eo[1] == o->eo[2] && force_form != 2) {
             size_t alt_smem = 0;
             ContourFn f = contour_alt_kernel_for(nx, o->eo[0], &alt_smem);
             if (f && alt_smem <= (size_t)dev_smem) {
@@ -1331,6 +1334,244 @@ int scft_diblock_time_phases(scft_diblock_t d, size_t n_iter, double out[4]) {
     for (int i = 0; i < 4; ++i) out[i] = n_iter ? acc[i] / (double)n_iter : 0.0;
     if (n_iter) d->last_iter_precision = d->precision;
     return diblock_check_device_error(d, st);
+}
+
+// ------------------------------- batches ----------------------------------
+// Many independent SCFT instances (own grid, cell, fA, chiN): one solver and one
+// iteration context each; one iteration of the whole batch is captured, fork-join over
+// worker streams, into a single CUDA graph, so the instances' contour kernels run
+// concurrently on the SMs.  The autotuner picks the number of worker streams and the
+// contour-kernel form per batch by timing.
+struct scft_batch_s {
+    int device = 0;
+    std::vector<scft_solver_t> solvers;
+    std::vector<scft_diblock_t> runs;
+    std::vector<cudaStream_t> streams;
+    std::vector<cudaEvent_t> joins;
+    cudaStream_t main = nullptr;
+    cudaEvent_t fork = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    size_t nstreams = 8;
+    int form = 0;
+
+    void drop_graph() {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        if (graph) cudaGraphDestroy(graph);
+        gexec = nullptr;
+        graph = nullptr;
+    }
+    ~scft_batch_s() {
+        if (main) cudaStreamSynchronize(main);
+        drop_graph();
+        for (auto r : runs) scft_diblock_destroy(r);
+        for (auto s : solvers) scft_solver_destroy(s);
+        for (auto e : joins) cudaEventDestroy(e);
+        if (fork) cudaEventDestroy(fork);
+        for (auto s : streams) cudaStreamDestroy(s);
+        if (main) cudaStreamDestroy(main);
+    }
+
+    int make_streams(size_t ns) {
+        for (auto e : joins) cudaEventDestroy(e);
+        for (auto s : streams) cudaStreamDestroy(s);
+        joins.clear();
+        streams.clear();
+        nstreams = std::max<size_t>(1, std::min(ns, runs.size()));
+        for (size_t i = 0; i < nstreams; ++i) {
+            cudaStream_t s;
+            cudaEvent_t e;
+            CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+            CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            streams.push_back(s);
+            joins.push_back(e);
+        }
+        return SCFT_OK;
+    }
+
+    int build_graph() {
+        drop_graph();
+        for (auto d : runs) {
+            d->force_form = form;
+            if (d->captured_gen == d->solver->ops_gen && d->last_form != form) d->captured_gen = ~0ULL;
+            d->last_form = form;
+            CKR(diblock_prepare(d, false));
+        }
+        CK(cudaStreamBeginCapture(main, cudaStreamCaptureModeThreadLocal));
+        int r = SCFT_OK;
+        cudaError_t e = cudaEventRecord(fork, main);
+        for (size_t w = 0; w < nstreams && e == cudaSuccess; ++w) e = cudaStreamWaitEvent(streams[w], fork, 0);
+        for (size_t i = 0; i < runs.size() && r == SCFT_OK && e == cudaSuccess; ++i)
+            r = runs[i]->enqueue(streams[i % nstreams]);
+        for (size_t w = 0; w < nstreams && e == cudaSuccess; ++w) {
+            e = cudaEventRecord(joins[w], streams[w]);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(main, joins[w], 0);
+        }
+        cudaGraph_t g = nullptr;
+        const cudaError_t e2 = cudaStreamEndCapture(main, &g);
+        if (r != SCFT_OK) {
+            if (g) cudaGraphDestroy(g);
+            return r;
+        }
+        if (e != cudaSuccess || e2 != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return fail(SCFT_ERR_CUDA, std::string("batch capture: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
+        }
+        graph = g;
+        CK(cudaGraphInstantiate(&gexec, graph, 0));
+        return SCFT_OK;
+    }
+
+    // n_iter iterations; per-iteration F and max incompressibility of every instance
+    int run(size_t n_iter, double* F, double* maxinc) {
+        if (!gexec) CKR(build_graph());
+        const size_t n = runs.size();
+        size_t done = 0;
+        std::vector<double> h;
+        while (done < n_iter) {
+            const size_t chunk = std::min<size_t>(n_iter - done, 1024);
+            IterState zero{};
+            for (auto d : runs) CK(cudaMemcpyAsync(d->state.p, &zero, sizeof(IterState), cudaMemcpyHostToDevice, main));
+            for (size_t k = 0; k < chunk; ++k) CK(cudaGraphLaunch(gexec, main));
+            for (size_t i = 0; i < n; ++i) {
+                scft_diblock_t d = runs[i];
+                h.resize(chunk * HIST_STRIDE);
+                CK(cudaMemcpyAsync(h.data(), d->hist.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, main));
+                CK(cudaStreamSynchronize(main));
+                for (size_t k = 0; k < chunk; ++k) {
+                    const double* rr = &h[k * HIST_STRIDE];
+                    if (F) F[(done + k) * n + i] = rr[HIST_F];
+                    if (maxinc) maxinc[(done + k) * n + i] = rr[HIST_MAXINC];
+                    if (rr[HIST_FLAGS] != 0.0) return fail(SCFT_ERR_NUMERIC, "instance " + std::to_string(i) + ": Q <= 0 or NaN");
+                }
+                CKR(diblock_check_device_error(d, main));
+                d->last_iter_precision = d->precision;
+            }
+            done += chunk;
+        }
+        return SCFT_OK;
+    }
+};
+
+int scft_batch_create(int kind, size_t n, const size_t* grid_log, const double* cell, const double* fA,
+                      const double* xN, double ds, double acceptance, int precision, int device,
+                      scft_batch_t* out) {
+    if (!out || !grid_log || !cell || !fA || !xN || n == 0) return fail(SCFT_ERR_INVALID_ARG, "null argument");
+    *out = nullptr;
+    auto b = std::make_unique<scft_batch_s>();
+    if (device < 0) CK(cudaGetDevice(&device));
+    b->device = device;
+    for (size_t i = 0; i < n; ++i) {
+        scft_solver_t s = nullptr;
+        CKR(scft_solver_create(kind, grid_log + 3 * i, nullptr, precision, device, &s));
+        b->solvers.push_back(s);
+        const double c6[6] = {cell[3 * i], cell[3 * i + 1], cell[3 * i + 2], 0, 0, 0};
+        CKR(scft_solver_set_cell_para(s, c6));
+        scft_diblock_t d = nullptr;
+        CKR(scft_diblock_create(s, fA[i], ds, xN[i], acceptance, &d));
+        b->runs.push_back(d);
+    }
+    CK(cudaSetDevice(device));
+    CK(cudaStreamCreateWithFlags(&b->main, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+    CKR(b->make_streams(8));
+    *out = b.release();
+    return SCFT_OK;
+}
+
+int scft_batch_destroy(scft_batch_t b) {
+    if (!b) return SCFT_OK;
+    cudaSetDevice(b->device);
+    delete b;
+    return SCFT_OK;
+}
+
+int scft_batch_size(scft_batch_t b, size_t* n) {
+    if (!b || !n) return fail(SCFT_ERR_INVALID_ARG, "null argument");
+    *n = b->runs.size();
+    return SCFT_OK;
+}
+
+int scft_batch_instance(scft_batch_t b, size_t i, scft_diblock_t* d) {
+    if (!b || !d || i >= b->runs.size()) return fail(SCFT_ERR_INVALID_ARG, "bad instance");
+    *d = b->runs[i];
+    return SCFT_OK;
+}
+
+int scft_batch_set_fields(scft_batch_t b, size_t i, const double* wA, const double* wB) {
+    if (!b || i >= b->runs.size()) return fail(SCFT_ERR_INVALID_ARG, "bad instance");
+    return scft_diblock_set_fields(b->runs[i], wA, wB);
+}
+
+int scft_batch_get_fields(scft_batch_t b, size_t i, double* phiA, double* phiB, double* wA, double* wB) {
+    if (!b || i >= b->runs.size()) return fail(SCFT_ERR_INVALID_ARG, "bad instance");
+    return scft_diblock_get_fields(b->runs[i], phiA, phiB, wA, wB);
+}
+
+int scft_batch_iterate(scft_batch_t b, size_t n_iter, double* F, double* maxinc) {
+    if (!b) return fail(SCFT_ERR_INVALID_ARG, "null handle");
+    for (auto d : b->runs)
+        if (!d->fields_set) return fail(SCFT_ERR_NOT_READY, "set the fields of every instance first");
+    CK(cudaSetDevice(b->device));
+    return b->run(n_iter, F, maxinc);
+}
+
+int scft_batch_configure(scft_batch_t b, size_t nstreams, int form) {
+    if (!b || form < 0 || form > 3) return fail(SCFT_ERR_INVALID_ARG, "bad configuration");
+    CK(cudaSetDevice(b->device));
+    CK(cudaStreamSynchronize(b->main));
+    b->drop_graph();
+    b->form = form;
+    return b->make_streams(nstreams);
+}
+
+int scft_batch_autotune(scft_batch_t b, size_t n_trial, size_t* best_nstreams, int* best_form, double* best_ms) {
+    if (!b || n_trial == 0) return fail(SCFT_ERR_INVALID_ARG, "bad argument");
+    CK(cudaSetDevice(b->device));
+    const size_t n = b->runs.size();
+    const size_t M0 = b->runs[0]->M;
+    (void)M0;
+    // the trials advance the fields: keep them and put them back afterwards
+    std::vector<std::vector<double>> keepA(n), keepB(n);
+    for (size_t i = 0; i < n; ++i) {
+        keepA[i].resize(b->runs[i]->M);
+        keepB[i].resize(b->runs[i]->M);
+        CKR(scft_diblock_get_fields(b->runs[i], nullptr, nullptr, keepA[i].data(), keepB[i].data()));
+    }
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    double best = 1e300;
+    size_t bs = b->nstreams;
+    int bf = b->form;
+    const size_t cand_streams[] = {2, 4, 8, 16, 32};
+    const int cand_forms[] = {0, 2};
+    for (int f : cand_forms) {
+        for (size_t ns : cand_streams) {
+            if (ns > n && ns != cand_streams[0]) continue;
+            CKR(scft_batch_configure(b, ns, f));
+            CKR(b->run(1, nullptr, nullptr));  // capture + warm up
+            CK(cudaEventRecord(e0, b->main));
+            CKR(b->run(n_trial, nullptr, nullptr));
+            CK(cudaEventRecord(e1, b->main));
+            CK(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, e0, e1));
+            if (ms < best) {
+                best = ms;
+                bs = ns;
+                bf = f;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    CKR(scft_batch_configure(b, bs, bf));
+    for (size_t i = 0; i < n; ++i) CKR(scft_diblock_set_fields(b->runs[i], keepA[i].data(), keepB[i].data()));
+    if (best_nstreams) *best_nstreams = bs;
+    if (best_form) *best_form = bf;
+    if (best_ms) *best_ms = best / (double)n_trial;
+    return SCFT_OK;
 }
 
 int scft_solver_set_stream(scft_solver_t s, void* stream) {

@@ -49,6 +49,7 @@ extern "C" {
 
 typedef struct scft_solver_s* scft_solver_t;
 typedef struct scft_diblock_s* scft_diblock_t;
+typedef struct scft_batch_s* scft_batch_t;
 
 /* Text of the last error on this host thread (static storage, never NULL). */
 const char* scft_last_error(void);
@@ -192,6 +193,34 @@ int scft_diblock_time_phases(scft_diblock_t d, size_t n_iter, double out[4]);
  * host threads) race and corrupt each other's results: serialise them. */
 #define SCFT_STATIC_SCRATCH_MAX_POINTS 262144
 int scft_solver_diffusion_device_static_scratch(scft_solver_t solver, double* d_io, void* stream);
+
+/* ========================================================================
+ * Batching form: many independent AB-diblock instances (each with its own grid,
+ * cell, fA and chiN; one solver kind, ds, mixing and precision for all) advanced
+ * together; one batch iteration is one CUDA-graph launch in which the instances'
+ * contour kernels run concurrently.  No counterpart in the reference (one instance
+ * per program run).
+ * ======================================================================== */
+
+/* grid_log: 3 n logical sizes; cell: 3 n lengths; fA, xN: n values each. */
+int scft_batch_create(int kind, size_t n, const size_t* grid_log, const double* cell, const double* fA,
+                      const double* xN, double ds, double acceptance, int precision, int device,
+                      scft_batch_t* out);
+int scft_batch_destroy(scft_batch_t b);
+int scft_batch_size(scft_batch_t b, size_t* n);
+/* The iteration context of instance i (owned by the batch; do not destroy). */
+int scft_batch_instance(scft_batch_t b, size_t i, scft_diblock_t* d);
+int scft_batch_set_fields(scft_batch_t b, size_t i, const double* wA, const double* wB);
+int scft_batch_get_fields(scft_batch_t b, size_t i, double* phiA, double* phiB, double* wA, double* wB);
+/* n_iter iterations of every instance; F and maxinc (may be NULL) get n_iter x n values,
+ * iteration-major. */
+int scft_batch_iterate(scft_batch_t b, size_t n_iter, double* F, double* maxinc);
+/* Worker streams and contour-kernel form (0 automatic, 1 alternating layout, 2 two-phase,
+ * 3 per-axis kernels). */
+int scft_batch_configure(scft_batch_t b, size_t nstreams, int form);
+/* Time n_trial batch iterations for each candidate configuration, keep the fastest
+ * (the fields are restored afterwards). */
+int scft_batch_autotune(scft_batch_t b, size_t n_trial, size_t* best_nstreams, int* best_form, double* best_ms);
 
 /* Measured FP64 throughput of `device` in TFLOP/s: FMA on the CUDA cores and
  * m8n8k4 MMA on the tensor cores (the denominator of the FP64 roofline).  No

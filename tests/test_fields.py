@@ -48,3 +48,16 @@ def test_layouts_follow_main():
 def test_contour_counts_truncate_like_the_reference(fA, ds, want):
     assert contour_counts(fA, ds) == want
     assert O.contour_counts(fA, ds) == want
+
+
+def test_batch_config_is_seeded_and_in_range():
+    from crysscft_sample_b200 import batch
+
+    a = batch.batch_config(64)
+    b = batch.batch_config(64)
+    assert a == b and len(a) == 64
+    for it in a:
+        assert it["N"][0] // 2 in (16, 24, 32, 48, 64)
+        assert 14.0 <= it["xN"] <= 30.0 and 0.2 <= it["fA"] <= 0.35 and 3.8 <= it["L"] <= 5.5
+        assert it["phase"] in ("BCC", "FCC")
+    assert len({it["N"] for it in a}) == 5
