@@ -57,6 +57,7 @@ SIGNATURES = {
     "scft_diblock_set_precision": (ctypes.c_int, [_vp, ctypes.c_int]),
     "scft_diblock_get_contour": (ctypes.c_int, [_vp, ctypes.c_int, _sz, _dp]),
     "scft_diblock_stress": (ctypes.c_int, [_vp, _dp, _dp, _dp]),
+    "scft_solver_set_pmmm_anisotropic": (ctypes.c_int, [_vp, ctypes.c_int]),
     "scft_batch_create": (ctypes.c_int, [ctypes.c_int, _sz, _szp, _dp, _dp, _dp, ctypes.c_double, ctypes.c_double,
                                          ctypes.c_int, ctypes.c_int, ctypes.POINTER(_vp)]),
     "scft_batch_destroy": (ctypes.c_int, [_vp]),

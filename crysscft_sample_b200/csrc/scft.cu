@@ -352,6 +352,7 @@ struct scft_solver_s {
     double* iomat = nullptr;  // pinned host buffer (get_iomat_for_diffusion)
     DevBuf<double> d_io, d_t1, d_t2;
     size_t launches = 0;
+    bool pmmm_anisotropic = false;  // PMMM with Lx, Ly, Lz (the reference's PMMM is cubic)
 
     ~scft_solver_s() {
         if (iomat) cudaFreeHost(iomat);
@@ -364,7 +365,7 @@ struct scft_solver_s {
             std::vector<long double> A;
             const int N = (int)grid_log[ax];
             if (kind == SCFT_SOLVER_PMMM)
-                A = pmmm_axis_operator(N / 2, (long double)cell[0], (long double)ds_);
+                A = pmmm_axis_operator(N / 2, (long double)cell[ax], (long double)ds_);
             else if (kind == SCFT_SOLVER_P1)
                 A = p1_axis_operator(N, (long double)cell[ax], (long double)ds_);
             else
@@ -394,7 +395,7 @@ struct scft_solver_s {
             const int n = (int)grid_phy[ax];
             std::vector<long double> A;
             if (kind == SCFT_SOLVER_PMMM)
-                A = pmmm_axis_operator_dL(N / 2, (long double)cell[0], (long double)ds);
+                A = pmmm_axis_operator_dL(N / 2, (long double)cell[ax], (long double)ds);
             else if (kind == SCFT_SOLVER_P1)
                 A = p1_axis_operator_dL(N, (long double)cell[ax], (long double)ds);
             else
@@ -839,11 +840,19 @@ int scft_solver_destroy(scft_solver_t s) {
     return SCFT_OK;
 }
 
+int scft_solver_set_pmmm_anisotropic(scft_solver_t s, int enable) {
+    if (!s) return fail(SCFT_ERR_INVALID_ARG, "null handle");
+    if (s->kind != SCFT_SOLVER_PMMM) return fail(SCFT_ERR_INVALID_ARG, "only the PMMM solver has a cubic restriction");
+    s->pmmm_anisotropic = enable != 0;
+    // takes effect at the next set_cell_para (the cell in use is kept as it is)
+    return SCFT_OK;
+}
+
 int scft_solver_set_cell_para(scft_solver_t s, const double c[6]) {
     if (!s || !c) return fail(SCFT_ERR_INVALID_ARG, "null argument");
     for (int i = 0; i < 3; ++i)
         if (!(c[i] > 0.0) || !std::isfinite(c[i])) return fail(SCFT_ERR_INVALID_ARG, "cell lengths must be > 0");
-    if (s->kind == SCFT_SOLVER_PMMM) {
+    if (s->kind == SCFT_SOLVER_PMMM && !s->pmmm_anisotropic) {
         // src/solver_Pmmm.h:98-104: cubic, only cell_para[0] is used
         const double c6[6] = {c[0], c[0], c[0], 0, 0, 0};
         std::memcpy(s->cell, c6, sizeof(c6));

@@ -80,6 +80,29 @@ def seed_fields(N, L, phase: str = "BCC", A: float = 2.0, sigma: float = 0.01, s
     return wA, wB
 
 
+def write_fields_text(path: str, phiA, phiB, wA, wB, precision: int = 6) -> None:
+    """The reference's output_fields format (src/crysSCFT_sample.cpp:271-282): one line
+    "phiA phiB wA wB" per grid point, x slowest, z fastest.  The reference streams doubles
+    with the default ostream format (6 significant digits, %g style); pass precision=17
+    for a lossless file."""
+    cols = [np.asarray(a, dtype=np.float64).ravel() for a in (phiA, phiB, wA, wB)]
+    fmt = f"%.{int(precision)}g"
+    with open(path, "w") as f:
+        for i in range(cols[0].size):
+            f.write(" ".join(fmt % c[i] for c in cols) + "\n")
+
+
+def read_fields_text(path: str, size: int):
+    """The reference's input_fields (src/crysSCFT_sample.cpp:284-292): reads `size` points
+    of "phiA phiB wA wB" (any whitespace); returns the four arrays."""
+    with open(path) as f:
+        vals = np.array(f.read().split()[: 4 * size], dtype=np.float64)
+    if vals.size < 4 * size:
+        raise ValueError(f"{path}: {vals.size // 4} points, expected {size}")
+    v = vals.reshape(size, 4)
+    return v[:, 0].copy(), v[:, 1].copy(), v[:, 2].copy(), v[:, 3].copy()
+
+
 def to_physical(kind: str, full: np.ndarray) -> np.ndarray:
     """main()'s per-solver field extraction (src/crysSCFT_sample.cpp:202-258)."""
     kind = kind.upper()

@@ -152,8 +152,11 @@ class CrysPSSolverPmmm(CrysPSSolverBase):
 
     _kind = "PMMM"
 
-    def __init__(self, grid_size_log, precision: str = "fp64", device: int = -1):
+    def __init__(self, grid_size_log, precision: str = "fp64", device: int = -1, anisotropic: bool = False):
         super().__init__(grid_size_log, None, precision, device)
+        if anisotropic:
+            # orthorhombic cell (Lx, Ly, Lz); the reference's PMMM solver is cubic
+            check(_lib.load().scft_solver_set_pmmm_anisotropic(self._h, 1))
 
 
 def make_solver(kind: str, grid_size_log, precision: str = "fp64", device: int = -1) -> CrysPSSolverBase:

@@ -78,6 +78,10 @@ int scft_solver_destroy(scft_solver_t solver);
  * As in the reference, PMMM uses cell_para[0] for all three axes
  * (src/solver_Pmmm.h:98-104); P1 and 3M use cell_para[0..2]. */
 int scft_solver_set_cell_para(scft_solver_t solver, const double cell_para[6]);
+/* PMMM with an orthorhombic cell: after enable = 1, set_cell_para uses Lx, Ly, Lz
+ * (cell_para[0..2]) instead of the reference's cubic cell_para[0] (src/solver_Pmmm.h:101).
+ * No counterpart in the reference; validated against P1 and 3M on the same cell. */
+int scft_solver_set_pmmm_anisotropic(scft_solver_t solver, int enable);
 /* CrysPSSolverBase::set_contour_step (src/solver_base.h:18).  Operators are cached per ds. */
 int scft_solver_set_contour_step(scft_solver_t solver, double ds);
 

@@ -92,6 +92,8 @@ def lib():
         L.ref_run_driver.argtypes = ([ctypes.c_void_p, ctypes.c_long, ctypes.c_long, ctypes.c_long]
                                      + [ctypes.c_double] * 7 + [ctypes.c_long, _dp, _dp,
                                                                 ctypes.c_char_p, ctypes.c_char_p, ctypes.c_long])
+        L.ref_output_fields.argtypes = [_dp] * 4 + [ctypes.c_long, ctypes.c_char_p]
+        L.ref_input_fields.argtypes = [_dp] * 4 + [ctypes.c_long, ctypes.c_char_p]
         L.ref_set_num_threads.argtypes = [ctypes.c_int]
         L.ref_get_max_threads.restype = ctypes.c_int
         _lib = L

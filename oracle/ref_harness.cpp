@@ -262,6 +262,15 @@ long ref_run_driver(void* h, long nx, long ny, long nz, double fA, double ds, do
     return (long)t;
 }
 
+// the reference's text field I/O (src/crysSCFT_sample.cpp:271-292)
+void ref_output_fields(const double* phiA, const double* phiB, const double* wA, const double* wB, long size,
+                       const char* filename) {
+    output_fields(phiA, phiB, wA, wB, (size_t)size, std::string(filename));
+}
+void ref_input_fields(double* phiA, double* phiB, double* wA, double* wB, long size, const char* filename) {
+    input_fields(phiA, phiB, wA, wB, (size_t)size, std::string(filename));
+}
+
 void ref_set_num_threads(int n) { omp_set_num_threads(n); }
 int ref_get_max_threads(void) { return omp_get_max_threads(); }
 
