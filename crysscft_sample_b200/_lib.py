@@ -28,6 +28,8 @@ SIGNATURES = {
     "scft_version": (ctypes.c_char_p, []),
     "scft_solver_create": (ctypes.c_int, [ctypes.c_int, _szp, _dp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_vp)]),
     "scft_solver_destroy": (ctypes.c_int, [_vp]),
+    "scft_operator_terms": (ctypes.c_int, [ctypes.c_int, _szp, _dp, _dp, ctypes.c_double,
+                                           ctypes.POINTER(ctypes.c_size_t), _dp, ctypes.c_size_t]),
     "scft_solver_set_cell_para": (ctypes.c_int, [_vp, _dp]),
     "scft_solver_set_contour_step": (ctypes.c_int, [_vp, ctypes.c_double]),
     "scft_solver_get_grid_size_log": (ctypes.c_int, [_vp, _szp]),

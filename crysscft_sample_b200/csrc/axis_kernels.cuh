@@ -8,6 +8,9 @@
 //   z pass: t1[o][i]       = sum_j A_z[i][j] (D q)[o][j]          (o = x*ny + y)
 //   y pass: t2[x][i][z]    = sum_j A_y[i][j] t1[x][j][z]
 //   x pass: q'[i][yz]      = D * sum_j A_x[i][j] t2[j][yz]
+// An operator that is a sum of Kronecker products runs the three passes once per
+// term; the x passes after the first add into q' (ChainIO::accum) and the last one
+// applies D.
 // Each pass is a batch of small GEMMs tiled through shared memory.  Both contour
 // chains of an SCFT iteration (forward q and backward q+) run in one launch
 // (blockIdx.z selects the chain).
@@ -22,6 +25,7 @@ struct ChainIO {
     T* out;
     const T* pre;   // multiply the input by pre[] elementwise (nullptr: no)
     const T* post;  // multiply the output by post[] elementwise (nullptr: no)
+    int accum = 0;  // add the pass result to what out[] holds (before post)
 };
 
 template <typename T>
@@ -112,6 +116,7 @@ axis_strided_kernel(const AxisPass<T> p) {
             if (gr >= inner) continue;
             const long long idx = (long long)gi * inner + gr;
             T v = acc[i][j];
+            if (io.accum) v = v + out[idx];
             if (post) v = v * post[idx];
             out[idx] = v;
         }
@@ -186,6 +191,7 @@ axis_contig_kernel(const AxisPass<T> p) {
             if (gi >= n) continue;
             const long long idx = go * n + gi;
             T v = acc[i][j];
+            if (io.accum) v = v + io.out[idx];
             if (io.post) v = v * io.post[idx];
             io.out[idx] = v;
         }

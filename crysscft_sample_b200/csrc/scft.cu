@@ -91,6 +91,12 @@ struct OpsSet {
     // cell-length derivatives dA/dL of the three axis operators (built on first use)
     DevBuf<double> d_dop[3], d_dopT[3];
     bool have_dop = false;
+    // an operator that is a sum of Kronecker products (3m with mirror translations):
+    // this set holds term 0, `more` the others (their d_op/f_op/d_dop only); the packed
+    // operators and the persistent contour kernels serve single-term operators only
+    int nterms = 1;
+    std::vector<std::unique_ptr<OpsSet>> more;
+    OpsSet* term(int t) { return t == 0 ? this : more[(size_t)t - 1].get(); }
 };
 
 // Round an FP32 value to the TF32 format (10 explicit mantissa bits), to nearest with
@@ -353,23 +359,36 @@ struct scft_solver_s {
     DevBuf<double> d_io, d_t1, d_t2;
     size_t launches = 0;
     bool pmmm_anisotropic = false;  // PMMM with Lx, Ly, Lz (the reference's PMMM is cubic)
+    M3Symmetry m3sym;                 // 3m mirror translations (decoded translational_part)
+    std::vector<M3Term> m3terms;      // its Kronecker terms (one when the translations are 0)
+    DevBuf<double> d_t3;              // input copy for in-place triplets of multi-term operators
 
     ~scft_solver_s() {
         if (iomat) cudaFreeHost(iomat);
         if (own_stream) cudaStreamDestroy(own_stream);
     }
 
+    int nterms() const { return kind == SCFT_SOLVER_3M ? (int)m3terms.size() : 1; }
+
     int build_ops(double ds_) {
         auto s = std::make_unique<OpsSet>();
+        const int nt = nterms();
+        s->nterms = nt;
+        for (int t = 1; t < nt; ++t) s->more.push_back(std::make_unique<OpsSet>());
         for (int ax = 0; ax < 3; ++ax) {
             std::vector<long double> A;
             const int N = (int)grid_log[ax];
-            if (kind == SCFT_SOLVER_PMMM)
+            if (kind == SCFT_SOLVER_PMMM) {
                 A = pmmm_axis_operator(N / 2, (long double)cell[ax], (long double)ds_);
-            else if (kind == SCFT_SOLVER_P1)
+            } else if (kind == SCFT_SOLVER_P1) {
                 A = p1_axis_operator(N, (long double)cell[ax], (long double)ds_);
-            else
-                A = m3_axis_operator(N, (long double)cell[ax], (long double)ds_);
+            } else {
+                const std::vector<long double> c = circulant_kernel(N, (long double)cell[ax], (long double)ds_);
+                for (int t = 1; t < nt; ++t)
+                    CKR(upload_operator(m3_axis_factor(c, N, m3sym.par[ax], m3terms[(size_t)t][ax]),
+                                        (int)grid_phy[ax], *s->term(t), ax));
+                A = m3_axis_factor(c, N, m3sym.par[ax], m3terms[0][ax]);
+            }
             CKR(upload_operator(A, (int)grid_phy[ax], *s, ax));
             pack_operator(A, (int)grid_phy[ax], *s, ax);
             pack_operator_f32(A, (int)grid_phy[ax], *s, ax);
@@ -393,23 +412,28 @@ struct scft_solver_s {
         for (int ax = 0; ax < 3; ++ax) {
             const int N = (int)grid_log[ax];
             const int n = (int)grid_phy[ax];
-            std::vector<long double> A;
-            if (kind == SCFT_SOLVER_PMMM)
-                A = pmmm_axis_operator_dL(N / 2, (long double)cell[ax], (long double)ds);
-            else if (kind == SCFT_SOLVER_P1)
-                A = p1_axis_operator_dL(N, (long double)cell[ax], (long double)ds);
-            else
-                A = m3_axis_operator_dL(N, (long double)cell[ax], (long double)ds);
-            std::vector<double> d((size_t)n * n), dt((size_t)n * n);
-            for (int i = 0; i < n; ++i)
-                for (int j = 0; j < n; ++j) {
-                    d[(size_t)i * n + j] = (double)A[(size_t)i * n + j];
-                    dt[(size_t)j * n + i] = (double)A[(size_t)i * n + j];
-                }
-            CKR(ops->d_dop[ax].alloc((size_t)n * n));
-            CKR(ops->d_dopT[ax].alloc((size_t)n * n));
-            CK(cudaMemcpy(ops->d_dop[ax].p, d.data(), d.size() * sizeof(double), cudaMemcpyHostToDevice));
-            CK(cudaMemcpy(ops->d_dopT[ax].p, dt.data(), dt.size() * sizeof(double), cudaMemcpyHostToDevice));
+            std::vector<long double> dc;
+            if (kind == SCFT_SOLVER_3M) dc = circulant_kernel_dL(N, (long double)cell[ax], (long double)ds);
+            for (int t = 0; t < ops->nterms; ++t) {
+                std::vector<long double> A;
+                if (kind == SCFT_SOLVER_PMMM)
+                    A = pmmm_axis_operator_dL(N / 2, (long double)cell[ax], (long double)ds);
+                else if (kind == SCFT_SOLVER_P1)
+                    A = p1_axis_operator_dL(N, (long double)cell[ax], (long double)ds);
+                else
+                    A = m3_axis_factor(dc, N, m3sym.par[ax], m3terms[(size_t)t][ax]);
+                std::vector<double> d((size_t)n * n), dt((size_t)n * n);
+                for (int i = 0; i < n; ++i)
+                    for (int j = 0; j < n; ++j) {
+                        d[(size_t)i * n + j] = (double)A[(size_t)i * n + j];
+                        dt[(size_t)j * n + i] = (double)A[(size_t)i * n + j];
+                    }
+                OpsSet* o = ops->term(t);
+                CKR(o->d_dop[ax].alloc((size_t)n * n));
+                CKR(o->d_dopT[ax].alloc((size_t)n * n));
+                CK(cudaMemcpy(o->d_dop[ax].p, d.data(), d.size() * sizeof(double), cudaMemcpyHostToDevice));
+                CK(cudaMemcpy(o->d_dopT[ax].p, dt.data(), dt.size() * sizeof(double), cudaMemcpyHostToDevice));
+            }
         }
         ops->have_dop = true;
         return SCFT_OK;
@@ -433,35 +457,44 @@ struct scft_solver_s {
     }
 
     // one triplet per chain: in -> (pre) z-pass -> t1 -> y-pass -> t2 -> x-pass (post) -> out
+    // A multi-term operator (ops->nterms > 1) runs the three passes per term and adds the
+    // x passes up in `out`, so there `in` and `out` must not alias.
     template <typename T>
     int triplet(int nchain, const ChainIO<T> io[2], T* t1[2], T* t2[2], cudaStream_t st) {
         const int nx = (int)grid_phy[0], ny = (int)grid_phy[1], nz = (int)grid_phy[2];
-        const T* opx;
-        const T* opy;
-        const T* opz;
-        const T* opxT;
-        const T* opyT;
-        const T* opzT;
-        if constexpr (sizeof(T) == 8) {
-            opx = (const T*)ops->d_op[0].p; opy = (const T*)ops->d_op[1].p; opz = (const T*)ops->d_op[2].p;
-            opxT = (const T*)ops->d_opT[0].p; opyT = (const T*)ops->d_opT[1].p; opzT = (const T*)ops->d_opT[2].p;
-        } else {
-            opx = (const T*)ops->f_op[0].p; opy = (const T*)ops->f_op[1].p; opz = (const T*)ops->f_op[2].p;
-            opxT = (const T*)ops->f_opT[0].p; opyT = (const T*)ops->f_opT[1].p; opzT = (const T*)ops->f_opT[2].p;
+        const int nt = ops->nterms;
+        for (int c = 0; c < nchain && nt > 1; ++c)
+            if ((const void*)io[c].in == (const void*)io[c].out)
+                return fail(SCFT_ERR_INVALID_ARG, "multi-term triplet: input and output alias");
+        for (int t = 0; t < nt; ++t) {
+            OpsSet* o = ops->term(t);
+            const T* opx;
+            const T* opy;
+            const T* opz;
+            const T* opxT;
+            const T* opyT;
+            const T* opzT;
+            if constexpr (sizeof(T) == 8) {
+                opx = (const T*)o->d_op[0].p; opy = (const T*)o->d_op[1].p; opz = (const T*)o->d_op[2].p;
+                opxT = (const T*)o->d_opT[0].p; opyT = (const T*)o->d_opT[1].p; opzT = (const T*)o->d_opT[2].p;
+            } else {
+                opx = (const T*)o->f_op[0].p; opy = (const T*)o->f_op[1].p; opz = (const T*)o->f_op[2].p;
+                opxT = (const T*)o->f_opT[0].p; opyT = (const T*)o->f_opT[1].p; opzT = (const T*)o->f_opT[2].p;
+            }
+            AxisPass<T> pz{}, py{}, px{};
+            for (int c = 0; c < nchain; ++c) {
+                pz.ch[c] = ChainIO<T>{io[c].in, t1[c], io[c].pre, nullptr};
+                py.ch[c] = ChainIO<T>{t1[c], t2[c], nullptr, nullptr};
+                px.ch[c] = ChainIO<T>{t2[c], io[c].out, nullptr, t == nt - 1 ? io[c].post : nullptr, t > 0};
+            }
+            pz.op = opz; pz.opT = opzT; pz.n = nz; pz.outer = (long long)nx * ny; pz.inner = 1;
+            py.op = opy; py.opT = opyT; py.n = ny; py.outer = nx; py.inner = nz;
+            px.op = opx; px.opT = opxT; px.n = nx; px.outer = 1; px.inner = (long long)ny * nz;
+            CK(launch_axis(pz, nchain, true, st));
+            CK(launch_axis(py, nchain, false, st));
+            CK(launch_axis(px, nchain, false, st));
+            launches += 3;
         }
-        AxisPass<T> pz{}, py{}, px{};
-        for (int c = 0; c < nchain; ++c) {
-            pz.ch[c] = ChainIO<T>{io[c].in, t1[c], io[c].pre, nullptr};
-            py.ch[c] = ChainIO<T>{t1[c], t2[c], nullptr, nullptr};
-            px.ch[c] = ChainIO<T>{t2[c], io[c].out, nullptr, io[c].post};
-        }
-        pz.op = opz; pz.opT = opzT; pz.n = nz; pz.outer = (long long)nx * ny; pz.inner = 1;
-        py.op = opy; py.opT = opyT; py.n = ny; py.outer = nx; py.inner = nz;
-        px.op = opx; px.opT = opxT; px.n = nx; px.outer = 1; px.inner = (long long)ny * nz;
-        CK(launch_axis(pz, nchain, true, st));
-        CK(launch_axis(py, nchain, false, st));
-        CK(launch_axis(px, nchain, false, st));
-        launches += 3;
         return SCFT_OK;
     }
 };
@@ -586,6 +619,7 @@ struct scft_diblock_s {
         persistent = false;
         alternating = false;
         if (force_form == 3) return SCFT_OK;  // per-axis kernels only
+        if (solver->ops && solver->ops->nterms > 1) return SCFT_OK;  // multi-term: per-axis kernels
         if (precision == SCFT_FP32) return setup_persistent_f32();
         const OpsSet* o = solver->ops;
         if (!o) return SCFT_OK;
@@ -804,10 +838,12 @@ int scft_solver_create(int kind, const size_t grid_size_log[3], const double tra
         return fail(SCFT_ERR_BAD_GRID, "ERROR: Grid Size Must Be Even For this symmetry");
     const size_t maxn = 1024;
     if (Nx > maxn || Ny > maxn || Nz > maxn) return fail(SCFT_ERR_BAD_GRID, "grid too large");
-    if (kind == SCFT_SOLVER_3M && translational_part)
-        for (int i = 0; i < 9; ++i)
-            if (translational_part[i] != 0.0)
-                return fail(SCFT_ERR_UNSUPPORTED, "3m solver: non-zero mirror translations are not supported yet");
+    M3Symmetry sym;
+    if (kind == SCFT_SOLVER_3M && translational_part) {
+        std::string why;
+        if (!m3_symmetry_from_g(translational_part, grid_size_log, &sym, &why))
+            return fail(SCFT_ERR_INVALID_ARG, "3m solver: " + why);
+    }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
         return fail(SCFT_ERR_NO_DEVICE, "no CUDA device");
@@ -823,12 +859,55 @@ int scft_solver_create(int kind, const size_t grid_size_log[3], const double tra
         s->grid_phy[i] = kind == SCFT_SOLVER_P1 ? grid_size_log[i] : grid_size_log[i] / 2;
     }
     s->M = s->grid_phy[0] * s->grid_phy[1] * s->grid_phy[2];
+    if (kind == SCFT_SOLVER_3M) {
+        s->m3sym = sym;
+        s->m3terms = m3_terms(sym);
+    }
     CK(cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking));
     s->stream = s->own_stream;
     cudaError_t e = cudaHostAlloc((void**)&s->iomat, s->M * sizeof(double), cudaHostAllocDefault);
     if (e != cudaSuccess) return fail(SCFT_ERR_ALLOC, "cudaHostAlloc iomat");
     std::memset(s->iomat, 0, s->M * sizeof(double));
     *out = s.release();
+    return SCFT_OK;
+}
+
+int scft_operator_terms(int kind, const size_t grid_size_log[3], const double translational_part[9],
+                        const double cell[3], double ds, size_t* nterms, double* factors, size_t capacity) {
+    if (!grid_size_log || !cell || !nterms) return fail(SCFT_ERR_INVALID_ARG, "null argument");
+    if (kind < SCFT_SOLVER_P1 || kind > SCFT_SOLVER_PMMM) return fail(SCFT_ERR_INVALID_ARG, "bad solver kind");
+    size_t N[3], n[3];
+    for (int a = 0; a < 3; ++a) {
+        N[a] = grid_size_log[a];
+        if (N[a] == 0 || N[a] > 1024) return fail(SCFT_ERR_BAD_GRID, "ERROR: Bad Grid Size");
+        if (kind != SCFT_SOLVER_P1 && N[a] % 2) return fail(SCFT_ERR_BAD_GRID, "ERROR: Grid Size Must Be Even");
+        if (!(cell[a] > 0.0)) return fail(SCFT_ERR_INVALID_ARG, "cell lengths must be > 0");
+        n[a] = kind == SCFT_SOLVER_P1 ? N[a] : N[a] / 2;
+    }
+    if (!(ds > 0.0)) return fail(SCFT_ERR_INVALID_ARG, "ds must be > 0");
+    std::vector<M3Term> terms(1);
+    M3Symmetry sym;
+    if (kind == SCFT_SOLVER_3M) {
+        if (translational_part) {
+            std::string why;
+            if (!m3_symmetry_from_g(translational_part, N, &sym, &why)) return fail(SCFT_ERR_INVALID_ARG, "3m solver: " + why);
+        }
+        terms = m3_terms(sym);
+    }
+    *nterms = terms.size();
+    if (!factors) return SCFT_OK;
+    const size_t need = terms.size() * (n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+    if (capacity < need) return fail(SCFT_ERR_INVALID_ARG, "factors: capacity too small");
+    double* o = factors;
+    for (size_t t = 0; t < terms.size(); ++t)
+        for (int a = 0; a < 3; ++a) {
+            std::vector<long double> A;
+            const long double L = (long double)cell[a], h = (long double)ds;
+            if (kind == SCFT_SOLVER_PMMM) A = pmmm_axis_operator((int)n[a], L, h);
+            else if (kind == SCFT_SOLVER_P1) A = p1_axis_operator((int)N[a], L, h);
+            else A = m3_axis_factor(circulant_kernel((int)N[a], L, h), (int)N[a], sym.par[a], terms[t][a]);
+            for (size_t i = 0; i < A.size(); ++i) *o++ = (double)A[i];
+        }
     return SCFT_OK;
 }
 
@@ -928,6 +1007,7 @@ static int ensure_work(scft_solver_t s) {
         CKR(s->d_t1.alloc(s->M));
         CKR(s->d_t2.alloc(s->M));
     }
+    if (s->nterms() > 1 && s->d_t3.n != s->M) CKR(s->d_t3.alloc(s->M));
     return SCFT_OK;
 }
 
@@ -938,7 +1018,12 @@ int scft_solver_diffusion_device(scft_solver_t s, double* d_io, void* stream) {
     CKR(ensure_work(s));
     cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
     ChainIO<double> io[2] = {{d_io, d_io, nullptr, nullptr}, {}};
-    // the z pass reads d_io into t1, the x pass writes d_io from t2: no aliasing inside a pass
+    // the z pass reads d_io into t1, the x pass writes d_io from t2: no aliasing inside a pass;
+    // a multi-term operator reads its input once per term, so it works from a copy
+    if (s->ops->nterms > 1) {
+        CK(cudaMemcpyAsync(s->d_t3.p, d_io, s->M * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        io[0].in = s->d_t3.p;
+    }
     double* t1[2] = {s->d_t1.p, nullptr};
     double* t2[2] = {s->d_t2.p, nullptr};
     return s->triplet<double>(1, io, t1, t2, st);
@@ -1145,13 +1230,17 @@ int scft_diblock_stress(scft_diblock_t d, double dlnQ_dL[3], double* dF_dxN, dou
     const int rblocks = (int)std::min<long long>(kRedMaxBlocks, (tc * M + kRedThreads - 1) / kRedThreads);
     std::vector<double> part(kRedMaxBlocks);
     for (int ax = 0; ax < 3; ++ax) {
+      double acc = 0.0;
+      // d/dL_a of a sum of Kronecker products: the sum over terms of each term with its
+      // axis-a factor replaced by the derivative factor
+      for (int term = 0; term < s->ops->nterms; ++term) {
+        const OpsSet* o = s->ops->term(term);
         const double* op[3];
         const double* opT[3];
         for (int b = 0; b < 3; ++b) {
-            op[b] = b == ax ? s->ops->d_dop[b].p : s->ops->d_op[b].p;
-            opT[b] = b == ax ? s->ops->d_dopT[b].p : s->ops->d_opT[b].p;
+            op[b] = b == ax ? o->d_dop[b].p : o->d_op[b].p;
+            opT[b] = b == ax ? o->d_dopT[b].p : o->d_opT[b].p;
         }
-        double acc = 0.0;
         for (int blk = 0; blk < 2; ++blk) {
             const long long lo = blk == 0 ? 0 : NsA, hi = blk == 0 ? NsA : U;
             const double* D = blk == 0 ? d->d_wAds.p : d->d_wBds.p;
@@ -1168,7 +1257,8 @@ int scft_diblock_stress(scft_diblock_t d, double dlnQ_dL[3], double* dF_dxN, dou
                 for (int i = 0; i < nb; ++i) acc += part[i];
             }
         }
-        if (dlnQ_dL) dlnQ_dL[ax] = acc / (double)M / Q;
+      }
+      if (dlnQ_dL) dlnQ_dL[ax] = acc / (double)M / Q;
     }
     if (dF_dxN) {
         // F (src/crysSCFT_sample.cpp:404-418) at fixed fields: d(xN <phiA phiB>)/dxN = <phiA phiB>,
@@ -1645,6 +1735,10 @@ extern "C" int scft_solver_diffusion_device_static_scratch(scft_solver_t s, doub
         }
         scratch = g_static_scratch_dev[s->device];
     }
+    if (s->ops->nterms > 1)
+        return fail(SCFT_ERR_UNSUPPORTED,
+                    "static-scratch triplet: a 3m solver with half-cell mirror translations needs a third scratch "
+                    "field; use scft_solver_diffusion_device");
     cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
     // the z pass writes every element of t1 before the y pass reads it, and the y pass
     // writes every element of t2 before the x pass reads it: nothing needs clearing

@@ -114,6 +114,41 @@ def to_physical(kind: str, full: np.ndarray) -> np.ndarray:
     return np.ascontiguousarray(full[:n0, :n1, :n2])
 
 
+def m3_mirror(b: int, p, g, N):
+    """The mirror normal to axis b of the 3m group with translations g
+    (generate_m3_operation, src/solver_utilities.h:56-66: g[0..2] belong to the mirror
+    normal to z, g[3..5] to y, g[6..8] to x), on integer grid coordinates p = (x, y, z):
+    p_b -> -p_b - 1 + g_b N_b (the plane lies between grid points), p_a -> p_a + g_a N_a."""
+    t = g[3 * (2 - b): 3 * (2 - b) + 3]
+    out = []
+    for a in range(3):
+        s = int(round(t[a] * N[a]))
+        out.append(((-p[a] - 1 + s) if a == b else (p[a] + s)) % N[a])
+    return tuple(out)
+
+
+def extend_3m(phy: np.ndarray, N, g=(0.0,) * 9) -> np.ndarray:
+    """The full-grid field of the 3m group with translations g whose even sub-lattice
+    f[2i, 2j, 2k] is `phy` (the 3m solver's physical grid): each of the eight group
+    elements m_x^cx m_y^cy m_z^cz (z applied first) carries the even sub-lattice onto one
+    parity class.  Raises if the translations do not tile the grid that way."""
+    N = tuple(int(v) for v in N)
+    phy = np.asarray(phy).reshape(tuple(v // 2 for v in N))
+    idx = np.meshgrid(*[2 * np.arange(v // 2) for v in N], indexing="ij")
+    full = np.empty(N, dtype=phy.dtype)
+    seen = np.zeros(N, dtype=np.int8)
+    for c in range(8):
+        p = tuple(idx)
+        for b, bit in ((2, 1), (1, 2), (0, 4)):
+            if c & bit:
+                p = m3_mirror(b, p, g, N)
+        full[p] = phy
+        seen[p] += 1
+    if not np.all(seen == 1):
+        raise ValueError("the mirror translations do not carry the even sub-lattice onto the other parity classes")
+    return full
+
+
 def from_physical(kind: str, phy: np.ndarray, N) -> np.ndarray:
     """Inverse of to_physical for mirror-symmetric fields."""
     kind = kind.upper()

@@ -165,6 +165,36 @@ def make_solver(kind: str, grid_size_log, precision: str = "fp64", device: int =
     return cls(grid_size_log, precision=precision, device=device)
 
 
+def operator_terms(kind: str, grid_size_log, cell, ds: float, translational_part=None):
+    """The per-axis factors [(A_x, A_y, A_z), ...] of the triplet the solver builds
+    (sum over terms of A_x (x) A_y (x) A_z on the physical grid).  Host-only: needs the
+    library but no GPU.  `cell` is used as given (also for PMMM)."""
+    L = _lib.load()
+    kind = kind.upper()
+    grid = (ctypes.c_size_t * 3)(*[int(v) for v in grid_size_log])
+    g = None
+    if translational_part is not None:
+        gg = np.ascontiguousarray(translational_part, dtype=np.float64)
+        if gg.size != 9:
+            raise ValueError("translational_part needs 9 values")
+        g = _lib.dptr(gg)
+    c = np.ascontiguousarray(cell[:3], dtype=np.float64)
+    nt = ctypes.c_size_t()
+    check(L.scft_operator_terms(_lib.KIND[kind], grid, g, _lib.dptr(c), float(ds), ctypes.byref(nt), None, 0))
+    n = [int(v) if kind == "P1" else int(v) // 2 for v in grid_size_log]
+    buf = np.zeros(nt.value * sum(v * v for v in n))
+    check(L.scft_operator_terms(_lib.KIND[kind], grid, g, _lib.dptr(c), float(ds), ctypes.byref(nt),
+                                _lib.dptr(buf), buf.size))
+    out, o = [], 0
+    for _ in range(nt.value):
+        fac = []
+        for v in n:
+            fac.append(buf[o:o + v * v].reshape(v, v))
+            o += v * v
+        out.append(tuple(fac))
+    return out
+
+
 def _check_tensor(t, n):
     import torch
 

@@ -65,14 +65,33 @@ const char* scft_version(void);
 /* Constructor.  Replaces CrysPSSolverP1(grid) (src/solver_p1.h:16-19),
  * CrysPSSolver3m(grid, translational_part) (src/solver_3m.h:17-20) and
  * CrysPSSolverPmmm(grid) (src/solver_Pmmm.h:16-19).  translational_part
- * (9 doubles, may be NULL = zeros) is used by SCFT_SOLVER_3M only; this build
- * supports the zero translation the reference's main() uses
- * (src/crysSCFT_sample.cpp:217) and returns SCFT_ERR_UNSUPPORTED otherwise.
+ * (9 doubles, may be NULL = zeros) is used by SCFT_SOLVER_3M only: the
+ * translations, in cell fractions, of the mirrors normal to z (g[0..2]), y (g[3..5])
+ * and x (g[6..8]), as in generate_m3_operation (src/solver_utilities.h:56-66).
+ * Accepted are the translations for which each mirror maps the even sub-lattice onto
+ * another parity class of the grid: components along other axes 0 or 1/2 (1/2 needs
+ * N % 4 == 0 on that axis), the component along the mirror normal an even number of
+ * grid points; anything else returns SCFT_ERR_INVALID_ARG.  Half-cell components make
+ * the triplet a sum of Kronecker products (see scft_operator_terms), which runs on the
+ * per-axis kernels instead of the persistent contour kernel.
  * device: CUDA ordinal (-1 = current device). */
 int scft_solver_create(int kind, const size_t grid_size_log[3], const double translational_part[9],
                        int precision, int device, scft_solver_t* out);
 /* Destructor (~CrysPSSolverP1 etc.).  NULL is accepted. */
 int scft_solver_destroy(scft_solver_t solver);
+
+/* Host-only, no device work (callable on a machine without a GPU): the per-axis
+ * factors of the triplet the solver of `kind` builds for grid_size_log,
+ * translational_part (as in scft_solver_create), cell lengths cell[0..2] (used as
+ * given, also for PMMM) and contour step ds.  The triplet on the physical grid is
+ * sum_t A_x^t (x) A_y^t (x) A_z^t.  *nterms receives the number of terms; when
+ * `factors` is not NULL it receives, term after term, A_x^t, A_y^t, A_z^t (row-major,
+ * n_a x n_a with n_a the physical axis length), provided `capacity` (doubles) holds
+ * them all.  No counterpart in the reference, which never forms these matrices
+ * (its triplets are src/solver_p1.h:184-202, src/solver_3m.h:281-324,
+ * src/solver_Pmmm.h:194-215). */
+int scft_operator_terms(int kind, const size_t grid_size_log[3], const double translational_part[9],
+                        const double cell[3], double ds, size_t* nterms, double* factors, size_t capacity);
 
 /* CrysPSSolverBase::set_cell_para (src/solver_base.h:16): {Lx,Ly,Lz,alpha,beta,gamma}.
  * As in the reference, PMMM uses cell_para[0] for all three axes
@@ -190,7 +209,8 @@ int scft_diblock_time_phases(scft_diblock_t d, size_t n_iter, double out[4]);
  * Scratch: a static device array inside the library of
  * 2 x SCFT_STATIC_SCRATCH_MAX_POINTS doubles (4 MiB), held by every GPU that loads
  * the library until the process exits.  Solvers with space_size_phy above
- * SCFT_STATIC_SCRATCH_MAX_POINTS are rejected with SCFT_ERR_INVALID_ARG.  The first
+ * SCFT_STATIC_SCRATCH_MAX_POINTS are rejected with SCFT_ERR_INVALID_ARG, and 3m
+ * solvers whose triplet has several Kronecker terms with SCFT_ERR_UNSUPPORTED.  The first
  * call on each device looks up the array's device address (cudaGetSymbolAddress);
  * make that first call before any stream capture.  All calls on a device share the
  * one array, so calls that overlap on the GPU (different streams, or different
