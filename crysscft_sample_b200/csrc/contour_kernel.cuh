@@ -17,6 +17,7 @@
 // every wait is bounded (spin limit), after which the kernel records an error and
 // returns, so a lost block can never hang the GPU.
 #pragma once
+#include <cuda.h>  // CUtensorMap (type only)
 #include <cuda_runtime.h>
 
 namespace crysscft {
@@ -43,7 +44,12 @@ struct ContourArgs {
     unsigned* bar_count;    // zeroed by the host before each launch
     int* error;             // bit 0: barrier wait gave up
     long long spin_limit;
-    unsigned* flags;        // alternating kernel: [chain][plane|slab][unit] last finished phase + 1, zeroed by the host
+    unsigned* flags;        // alternating kernel: [chain][plane|slab][consumer][producer] last finished phase + 1, zeroed by the host
+    // alternating kernel: TMA descriptors of the slab-layout tiles (an nx x nz tile at fixed y):
+    // the contour store of each chain as (z, y, x, slot) with box (nz, 1, nx, 1), and the
+    // Boltzmann factors of blocks A and B as (z, y, x) with box (nz, 1, nx)
+    alignas(64) CUtensorMap tm_qs[2];
+    alignas(64) CUtensorMap tm_ws[2];
 };
 
 __device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
@@ -627,6 +633,65 @@ __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src)
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
+// ---- bulk-copy engine (cp.async.bulk, no tensor map) and mbarriers ----------------
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_test(unsigned long long* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Wait for the phase of `bar` with the given parity to complete; false after `limit` polls.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, long long limit) {
+    long long spins = 0;
+    while (!mbar_test(bar, parity)) {
+        if (++spins > limit) return false;
+    }
+    return true;
+}
+// global -> shared bulk copy (16-byte aligned, size a multiple of 16) completing on `bar`
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+// shared -> global bulk copy, tracked by the issuing thread's bulk groups
+__device__ __forceinline__ void bulk_store(void* dst, const void* src, unsigned bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// the source shared memory of this thread's bulk stores may be overwritten after this
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+// generic-proxy shared-memory writes become visible to the bulk-copy engine
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// tiled TMA: 3-D box at (c0, c1, c2) into shared memory, completing on `bar`
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1, int c2,
+                                            unsigned long long* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+        ::"r"(smem_u32(dst)), "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+        : "memory");
+}
+// tiled TMA: shared memory to the 4-D box at (c0, c1, c2, c3), tracked by bulk groups
+__device__ __forceinline__ void tma_store_4d(const CUtensorMap* map, const void* src, int c0, int c1, int c2, int c3) {
+    asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group [%0, {%2, %3, %4, %5}], [%1];"
+                 ::"l"(map), "r"(smem_u32(src)), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+                 : "memory");
+}
+
 // N x N tile from global (row stride gs) into shared memory (row stride LF) with cp.async
 template <int N, int LF>
 __device__ __forceinline__ void tile_fetch(double* sm, const double* gm, long long gs) {
@@ -651,7 +716,7 @@ __device__ __forceinline__ void tile_store(const double* sm, double* gm, long lo
     }
 }
 
-// T <- T * W (elementwise on an N x N tile in shared memory)
+// T <- T * W (T row stride LF, W dense N x N)
 template <int N, int LF>
 __device__ __forceinline__ void tile_scale(double* T, const double* W) {
     constexpr int PER_ROW = N / 2;
@@ -660,29 +725,29 @@ __device__ __forceinline__ void tile_scale(double* T, const double* W) {
     for (int e = threadIdx.x; e < TOTAL; e += kContourThreads) {
         const int r = e / PER_ROW, c = (e - r * PER_ROW) * 2;
         double2 v = *reinterpret_cast<double2*>(T + r * LF + c);
-        const double2 w = *reinterpret_cast<const double2*>(W + r * LF + c);
+        const double2 w = *reinterpret_cast<const double2*>(W + r * N + c);
         v.x = v.x * w.x;
         v.y = v.y * w.y;
         *reinterpret_cast<double2*>(T + r * LF + c) = v;
     }
 }
 
-// v = T * W0 stored to global (the finished q(s+1)); if start, T <- v * W1 (D of the next step)
+// v = T * W0 into the dense staging tile QS (the finished q(s+1), stored from there by
+// the bulk-copy engine); if start, T <- v * W1 (D of the next step)
 template <int N, int LF>
-__device__ __forceinline__ void tile_finish(double* T, const double* W0, const double* W1, double* gm,
-                                            long long gs, bool start) {
+__device__ __forceinline__ void tile_finish(double* T, const double* W0, const double* W1, double* QS, bool start) {
     constexpr int PER_ROW = N / 2;
     constexpr int TOTAL = N * PER_ROW;
 #pragma unroll 4
     for (int e = threadIdx.x; e < TOTAL; e += kContourThreads) {
         const int r = e / PER_ROW, c = (e - r * PER_ROW) * 2;
         double2 v = *reinterpret_cast<double2*>(T + r * LF + c);
-        const double2 w0 = *reinterpret_cast<const double2*>(W0 + r * LF + c);
+        const double2 w0 = *reinterpret_cast<const double2*>(W0 + r * N + c);
         v.x = v.x * w0.x;
         v.y = v.y * w0.y;
-        *reinterpret_cast<double2*>(gm + r * gs + c) = v;
+        *reinterpret_cast<double2*>(QS + r * N + c) = v;
         if (start) {
-            const double2 w1 = *reinterpret_cast<const double2*>(W1 + r * LF + c);
+            const double2 w1 = *reinterpret_cast<const double2*>(W1 + r * N + c);
             v.x = v.x * w1.x;
             v.y = v.y * w1.y;
             *reinterpret_cast<double2*>(T + r * LF + c) = v;
@@ -690,151 +755,237 @@ __device__ __forceinline__ void tile_finish(double* T, const double* W0, const d
     }
 }
 
+// Shared-memory carve-up of the alternating kernel: operators, two padded work tiles
+// (row stride LF, conflict-free MMA fragments), and three dense N x N tiles filled and
+// drained by the bulk-copy engine (Boltzmann factors W0/W1, q staging tile QS).
 template <int N, bool EO>
 struct AltShape {
     static constexpr int LF = N + 4;
     static constexpr int OPS = 3 * AxisShape<N, EO>::SIZE;
-    static constexpr int OPS_PAD = (OPS + 1) & ~1;
-    static constexpr int TILE = N * LF;
-    static constexpr size_t SMEM = (size_t)(OPS_PAD + 4 * TILE) * sizeof(double);
+    static constexpr int OPS_PAD = (OPS + 15) & ~15;        // 128-byte aligned tiles after it
+    static constexpr int TILE = (N * LF + 15) & ~15;
+    static constexpr int WT = N * N;
+    // + 128: the carve-up starts at the first 128-byte boundary of the dynamic window
+    static constexpr size_t SMEM = (size_t)(OPS_PAD + 2 * TILE + 3 * WT) * sizeof(double) + 128;
 };
 
 __device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+// Preconditions of the bulk/TMA copies, checked once per launch before any is issued:
+// bit 3 of the returned word: a shared-memory tile not 128-byte aligned; bit 4: a TMA
+// descriptor not 64-byte aligned.  0 when every copy may be issued.
+__device__ __forceinline__ int tma_alignment_error(const void* const* tiles, int ntiles, const CUtensorMap* maps,
+                                                   int nmaps) {
+    int e = 0;
+    for (int i = 0; i < ntiles; ++i)
+        if (smem_u32(tiles[i]) & 127u) e |= 8;
+    for (int i = 0; i < nmaps; ++i)
+        if (reinterpret_cast<uintptr_t>(&maps[i]) & 63u) e |= 16;
+    return e;
+}
+
+// Lane 0 of warp 0 loads one N x N Boltzmann-factor tile: a plane (contiguous, one bulk
+// copy) or a slab (N rows of stride N^2: one tiled TMA box through `slab_map`).
+template <typename T, int N>
+__device__ __forceinline__ void bulk_tile_load(T* dst, const T* src, int p, bool plane, const CUtensorMap* slab_map,
+                                               unsigned long long* bar) {
+    if ((threadIdx.x & 31) != 0) return;
+    if (plane) bulk_load(dst, src + (long long)p * N * N, (unsigned)(N * N * sizeof(T)), bar);
+    else tma_load_3d(dst, slab_map, 0, p, 0, bar);
+}
+
+// Lane 0 of warp 0 stores the dense staging tile QS to contour slot `slot`: a plane
+// (contiguous, one bulk copy) or a slab (one tiled TMA box through `slab_map`), and
+// commits it as one bulk group.
+template <typename T, int N>
+__device__ __forceinline__ void bulk_tile_store(T* q, const T* QS, int p, long long slot, bool plane,
+                                                const CUtensorMap* slab_map) {
+    if ((threadIdx.x & 31) != 0) return;
+    constexpr long long M = (long long)N * N * N;
+    if (plane) bulk_store(q + slot * M + (long long)p * N * N, QS, (unsigned)(N * N * sizeof(T)));
+    else tma_store_4d(slab_map, QS, 0, p, 0, (int)slot);
+    bulk_commit();
+}
+
 template <int N, bool EO>
-__global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const ContourArgs a) {
+__global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const __grid_constant__ ContourArgs a) {
     using S = AltShape<N, EO>;
     constexpr int LF = S::LF;
     constexpr int OFFY = AxisShape<N, EO>::SIZE;
     constexpr int OFFZ = 2 * AxisShape<N, EO>::SIZE;
     constexpr int TPR = kContourThreads / N;         // threads per tile row (rows * TPR <= block)
     constexpr int CPT = (N / 2 + TPR - 1) / TPR;     // 16-byte chunks per thread and row
+    constexpr unsigned TILE_BYTES = N * N * sizeof(double);
     static_assert(TPR >= 1, "tile rows must not exceed the block");
-    extern __shared__ __align__(16) double smem[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    // the dynamic window is only guaranteed 16-byte alignment; TMA tiles need 128
+    double* smem = reinterpret_cast<double*>(smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u));
     double* sops = smem;
     double* T0 = smem + S::OPS_PAD;
     double* T1 = T0 + S::TILE;
     double* W0 = T1 + S::TILE;  // D of the step being finished
-    double* W1 = W0 + S::TILE;  // D of the step being started
+    double* W1 = W0 + S::WT;    // D of the step being started
+    double* QS = W1 + S::WT;    // finished q(s+1), drained by bulk stores
+    __shared__ __align__(8) unsigned long long s_bar;  // completion of the W0/W1 bulk loads
     __shared__ int s_fail;
-    for (int i = threadIdx.x; i < S::OPS; i += kContourThreads) sops[i] = a.ops[i];
-    if (threadIdx.x == 0) s_fail = 0;
 
     constexpr long long M = (long long)N * N * N;
     constexpr long long PLANE = (long long)N * N;
     const int units = a.nchain * N;
-    const int U = a.t_end;  // steps 0..U-1 of both chains (t_begin is 0)
+    const int u = blockIdx.x;  // one unit per block: the host launches units <= SMs blocks
+    if (units > (int)gridDim.x) {
+        if (threadIdx.x == 0) atomicOr(a.error, 4);
+        return;
+    }
+    if (u >= units) return;
+    const int warp = threadIdx.x >> 5;
+    {
+        const void* tiles[3] = {W0, W1, QS};
+        const int e = tma_alignment_error(tiles, 3, a.tm_qs, 2) | tma_alignment_error(tiles, 0, a.tm_ws, 2);
+        if (e) {
+            if (threadIdx.x == 0) atomicOr(a.error, e);
+            return;
+        }
+    }
+    for (int i = threadIdx.x; i < S::OPS; i += kContourThreads) sops[i] = a.ops[i];
+    if (threadIdx.x == 0) {
+        s_fail = 0;
+        mbar_init(&s_bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
 
-    // exp(-w ds/2) of step s of chain c: block A for segments < NsA, else block B
-    auto w_of = [&](int c, int s) -> const double* {
-        const int dir = c ? a.dir[1] : a.dir[0];
-        const long long in_slot = (c ? a.slot0[1] : a.slot0[0]) + (long long)dir * s;
+    const int U = a.t_end;  // steps 0..U-1 of both chains (t_begin is 0)
+    const int c = u >= N ? 1 : 0, p = u - c * N;
+    const int dir = c ? a.dir[1] : a.dir[0];
+    const long long slot0 = c ? a.slot0[1] : a.slot0[0];
+    double* q = c ? a.q[1] : a.q[0];
+    double* XP = c ? a.xbuf[1] : a.xbuf[0];  // written by plane phases
+    double* XS = XP + M;                     // written by slab phases
+    // flags[chain][producing layout][consumer][producer]: every consumer polls its own
+    // N flags (one cache line per 32), written by the producers (push), so the waits of
+    // different blocks never share a line
+    unsigned* fl_plane = a.flags + (size_t)c * 2 * N * N;  // written by plane units
+    unsigned* fl_slab = fl_plane + (size_t)N * N;           // written by slab units
+
+    // block of the Boltzmann factor exp(-w ds/2) of step s: A (0) for segments < NsA, else B (1)
+    auto blk_of = [&](int s) -> int {
+        const long long in_slot = slot0 + (long long)dir * s;
         const long long seg = dir > 0 ? in_slot : in_slot - 1;
-        return seg < a.NsA ? a.wds[0] : a.wds[1];
+        return seg < a.NsA ? 0 : 1;
     };
-    // cp.async the Boltzmann slices phase k of unit u needs (plane: x-plane; slab: y-row)
-    auto fetch_w = [&](int k, int u) {
-        const int c = u >= N ? 1 : 0, p = u - c * N;
+    // warp 0: bulk-load the Boltzmann tiles of phase k (W0 = D of step k-1, W1 = D of step k)
+    auto issue_w = [&](int k) {
+        const bool plane = (k & 1) == 0;
+        const unsigned bytes = ((k >= 1) + (k < U)) * TILE_BYTES;
+        if ((threadIdx.x & 31) == 0) mbar_expect_tx(&s_bar, bytes);
+        __syncwarp();
+        if (k >= 1) bulk_tile_load<double, N>(W0, a.wds[blk_of(k - 1)], p, plane, &a.tm_ws[blk_of(k - 1)], &s_bar);
+        if (k < U) bulk_tile_load<double, N>(W1, a.wds[blk_of(k)], p, plane, &a.tm_ws[blk_of(k)], &s_bar);
+    };
+    unsigned wpar = 0;  // parity of the pending W phase of s_bar
+    // error exit: let this block's bulk copies finish (bounded), then return
+    auto drain = [&](bool w_pending) {
+        if (w_pending) mbar_wait(&s_bar, wpar, a.spin_limit);
+        if (warp == 0) bulk_wait_all();
+    };
+
+    if (warp == 0) issue_w(0);
+    for (int k = 0; k <= U; ++k) {
         const bool plane = (k & 1) == 0;
         const long long off = plane ? (long long)p * PLANE : (long long)p * N;
         const long long gs = plane ? N : PLANE;
-        if (k >= 1) tile_fetch<N, LF>(W0, w_of(c, k - 1) + off, gs);
-        if (k < U) tile_fetch<N, LF>(W1, w_of(c, k) + off, gs);
-        cp_async_commit();
-    };
-
-    if ((int)blockIdx.x < units) fetch_w(0, blockIdx.x);
-    for (int k = 0; k <= U; ++k) {
-        const bool plane = (k & 1) == 0;
-        for (int u = blockIdx.x; u < units; u += gridDim.x) {
-            const int c = u >= N ? 1 : 0, p = u - c * N;
-            const int dir = c ? a.dir[1] : a.dir[0];
-            const long long slot0 = c ? a.slot0[1] : a.slot0[0];
-            double* q = c ? a.q[1] : a.q[0];
-            double* XP = c ? a.xbuf[1] : a.xbuf[0];  // written by plane phases
-            double* XS = XP + M;                     // written by slab phases
-            unsigned* fl_plane = a.flags + (size_t)c * 2 * N;
-            unsigned* fl_slab = fl_plane + N;
-            const long long off = plane ? (long long)p * PLANE : (long long)p * N;
-            const long long gs = plane ? N : PLANE;
-            if (u != (int)blockIdx.x) fetch_w(k, u);  // more units than blocks
-            if (k == 0) {
-                tile_fetch<N, LF>(T0, q + slot0 * M + off, gs);
-            } else {
-                // row r of this tile was produced by unit r of the other layout in phase k-1:
-                // wait for its flag, then fetch the row (waits and copies overlap)
-                const int r = threadIdx.x / TPR, sub = threadIdx.x - r * TPR;
-                if (r < N) {
-                    const unsigned* f = plane ? fl_slab + r : fl_plane + r;
-                    long long spins = 0;
-                    while (ld_acquire_u32(f) < (unsigned)k) {
-                        if (++spins > a.spin_limit) {
-                            atomicOr(a.error, 1);
-                            s_fail = 1;
-                            break;
-                        }
-                        if (spins > 64) __nanosleep(20);
+        if (k == 0) {
+            tile_fetch<N, LF>(T0, q + slot0 * M + off, gs);
+        } else {
+            // row r of this tile was produced by unit r of the other layout in phase k-1:
+            // wait for its flag, then fetch the row (waits and copies overlap)
+            const int r = threadIdx.x / TPR, sub = threadIdx.x - r * TPR;
+            if (r < N) {
+                const unsigned* f = (plane ? fl_slab : fl_plane) + (size_t)p * N + r;
+                long long spins = 0;
+                while (ld_acquire_u32(f) < (unsigned)k) {
+                    if (++spins > a.spin_limit) {
+                        atomicOr(a.error, 1);
+                        s_fail = 1;
+                        break;
                     }
-                    const double* src = (plane ? XS : XP) + off + r * gs;
+                    if (spins > 64) __nanosleep(20);
+                }
+                const double* src = (plane ? XS : XP) + off + r * gs;
 #pragma unroll
-                    for (int j = 0; j < CPT; ++j) {
-                        const int ch = sub + j * TPR;
-                        if (ch < N / 2) cp_async16(T0 + r * LF + 2 * ch, src + 2 * ch);
-                    }
+                for (int j = 0; j < CPT; ++j) {
+                    const int ch = sub + j * TPR;
+                    if (ch < N / 2) cp_async16(T0 + r * LF + 2 * ch, src + 2 * ch);
                 }
             }
-            cp_async_commit();
-            cp_async_wait_all();
-            __syncthreads();
-            if (s_fail) return;
-            double* cur = T0;
-            double* oth = T1;
-            if (k >= 1) {
-                // finish step k-1: the axis ops this layout owns, then D, store q
-                if (plane) {
-                    row_op_ct<N, N, LF, EO>(cur, oth, sops + OFFZ);
-                    __syncthreads();
-                    col_op_ct<N, N, LF, EO>(oth, cur, sops + OFFY);
-                } else {
-                    col_op_ct<N, N, LF, EO>(cur, oth, sops);
-                    double* tmp = cur;
-                    cur = oth;
-                    oth = tmp;
-                }
+        }
+        cp_async_commit();
+        cp_async_wait_all();
+        __syncthreads();
+        if (s_fail) {
+            drain(true);
+            return;
+        }
+        double* cur = T0;
+        double* oth = T1;
+        if (k >= 1) {
+            // finish step k-1: the axis ops this layout owns, then D, store q
+            if (plane) {
+                row_op_ct<N, N, LF, EO>(cur, oth, sops + OFFZ);
                 __syncthreads();
-                const long long out_slot = slot0 + (long long)dir * k;
-                tile_finish<N, LF>(cur, W0, W1, q + out_slot * M + off, gs, k < U);
+                col_op_ct<N, N, LF, EO>(oth, cur, sops + OFFY);
             } else {
-                tile_scale<N, LF>(cur, W1);
+                col_op_ct<N, N, LF, EO>(cur, oth, sops);
+                double* tmp = cur;
+                cur = oth;
+                oth = tmp;
             }
+            if (warp == 0) bulk_wait_read();  // the previous q store has left QS
+        }
+        const bool w_ok = mbar_wait(&s_bar, wpar, a.spin_limit);
+        wpar ^= 1u;
+        if (!w_ok) {
+            if (threadIdx.x == 0) atomicOr(a.error, 2);
+            if (warp == 0) bulk_wait_all();
+            return;
+        }
+        __syncthreads();
+        if (k >= 1) {
+            tile_finish<N, LF>(cur, W0, W1, QS, k < U);
+            fence_async_smem();
             __syncthreads();
-            if (k < U) {
-                // start step k on this layout; the other layout finishes it next phase
-                if (plane) {
-                    row_op_ct<N, N, LF, EO>(cur, oth, sops + OFFZ);
-                    __syncthreads();
-                    col_op_ct<N, N, LF, EO>(oth, cur, sops + OFFY);
-                } else {
-                    col_op_ct<N, N, LF, EO>(cur, oth, sops);
-                    double* tmp = cur;
-                    cur = oth;
-                    oth = tmp;
-                }
-                __syncthreads();
-                tile_store<N, LF>(cur, (plane ? XP : XS) + off, gs);
-                __syncthreads();
-                if (threadIdx.x == 0) {
-                    __threadfence();
-                    st_release_u32((plane ? fl_plane : fl_slab) + p, (unsigned)(k + 1));
-                }
-            }
+            if (warp == 0) bulk_tile_store<double, N>(q, QS, p, slot0 + (long long)dir * k, plane, &a.tm_qs[c]);
+        } else {
+            tile_scale<N, LF>(cur, W1);
             __syncthreads();
         }
-        if (k < U && (int)blockIdx.x < units) fetch_w(k + 1, blockIdx.x);  // overlaps the next waits
+        if (k < U) {
+            if (warp == 0) issue_w(k + 1);  // W0/W1 are free: prefetch the next phase's factors
+            // start step k on this layout; the other layout finishes it next phase
+            if (plane) {
+                row_op_ct<N, N, LF, EO>(cur, oth, sops + OFFZ);
+                __syncthreads();
+                col_op_ct<N, N, LF, EO>(oth, cur, sops + OFFY);
+            } else {
+                col_op_ct<N, N, LF, EO>(cur, oth, sops);
+                double* tmp = cur;
+                cur = oth;
+                oth = tmp;
+            }
+            __syncthreads();
+            tile_store<N, LF>(cur, (plane ? XP : XS) + off, gs);
+            __syncthreads();
+            if (threadIdx.x < N) {  // tell consumer threadIdx.x that tile p of phase k is out
+                __threadfence();
+                st_release_u32((plane ? fl_plane : fl_slab) + (size_t)threadIdx.x * N + p, (unsigned)(k + 1));
+            }
+        }
+        __syncthreads();
     }
-    cp_async_wait_all();
+    if (warp == 0) bulk_wait_all();
 }
 
 }  // namespace crysscft

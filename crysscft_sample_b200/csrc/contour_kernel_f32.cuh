@@ -261,6 +261,7 @@ __device__ __forceinline__ void tile_store_f32(const float* sm, float* gm, long 
         *reinterpret_cast<float4*>(gm + r * gs + c) = *reinterpret_cast<const float4*>(sm + r * LF + c);
     }
 }
+// T <- T * W (T row stride LF, W dense N x N)
 template <int N, int LF>
 __device__ __forceinline__ void tile_scale_f32(float* T, const float* W) {
     constexpr int PER_ROW = N / 4;
@@ -269,7 +270,7 @@ __device__ __forceinline__ void tile_scale_f32(float* T, const float* W) {
     for (int e = threadIdx.x; e < TOTAL; e += kContourThreads) {
         const int r = e / PER_ROW, c = (e - r * PER_ROW) * 4;
         float4 v = *reinterpret_cast<float4*>(T + r * LF + c);
-        const float4 w = *reinterpret_cast<const float4*>(W + r * LF + c);
+        const float4 w = *reinterpret_cast<const float4*>(W + r * N + c);
         v.x *= w.x;
         v.y *= w.y;
         v.z *= w.z;
@@ -277,23 +278,24 @@ __device__ __forceinline__ void tile_scale_f32(float* T, const float* W) {
         *reinterpret_cast<float4*>(T + r * LF + c) = v;
     }
 }
+// v = T * W0 into the dense staging tile QS (stored by the bulk-copy engine); if start,
+// T <- v * W1 (D of the next step)
 template <int N, int LF>
-__device__ __forceinline__ void tile_finish_f32(float* T, const float* W0, const float* W1, float* gm, long long gs,
-                                                bool start) {
+__device__ __forceinline__ void tile_finish_f32(float* T, const float* W0, const float* W1, float* QS, bool start) {
     constexpr int PER_ROW = N / 4;
     constexpr int TOTAL = N * PER_ROW;
 #pragma unroll 4
     for (int e = threadIdx.x; e < TOTAL; e += kContourThreads) {
         const int r = e / PER_ROW, c = (e - r * PER_ROW) * 4;
         float4 v = *reinterpret_cast<float4*>(T + r * LF + c);
-        const float4 w0 = *reinterpret_cast<const float4*>(W0 + r * LF + c);
+        const float4 w0 = *reinterpret_cast<const float4*>(W0 + r * N + c);
         v.x *= w0.x;
         v.y *= w0.y;
         v.z *= w0.z;
         v.w *= w0.w;
-        *reinterpret_cast<float4*>(gm + r * gs + c) = v;
+        *reinterpret_cast<float4*>(QS + r * N + c) = v;
         if (start) {
-            const float4 w1 = *reinterpret_cast<const float4*>(W1 + r * LF + c);
+            const float4 w1 = *reinterpret_cast<const float4*>(W1 + r * N + c);
             v.x *= w1.x;
             v.y *= w1.y;
             v.z *= w1.z;
@@ -303,13 +305,18 @@ __device__ __forceinline__ void tile_finish_f32(float* T, const float* W0, const
     }
 }
 
+// Shared memory: operators, two padded work tiles, the four Boltzmann-factor tiles of
+// this block's unit (blocks A and B, plane and slab layout; loaded once per launch),
+// and the dense q staging tile.
 template <int N, bool EO>
 struct AltShapeF {
     static constexpr int LF = N + 4;
     static constexpr int OPS = 3 * AxisShapeF<N, EO>::SIZE;
-    static constexpr int OPS_PAD = (OPS + 3) & ~3;
-    static constexpr int TILE = N * LF;
-    static constexpr size_t SMEM = (size_t)(OPS_PAD + 4 * TILE) * sizeof(float);
+    static constexpr int OPS_PAD = (OPS + 31) & ~31;  // 128-byte aligned tiles after it
+    static constexpr int TILE = (N * LF + 31) & ~31;
+    static constexpr int WT = N * N;
+    // + 128: the carve-up starts at the first 128-byte boundary of the dynamic window
+    static constexpr size_t SMEM = (size_t)(OPS_PAD + 2 * TILE + 5 * WT) * sizeof(float) + 128;
 };
 
 struct ContourArgsF {
@@ -324,135 +331,173 @@ struct ContourArgsF {
     int t_end;
     int* error;
     long long spin_limit;
-    unsigned* flags;       // [chain][plane|slab][unit], zeroed by the host
+    unsigned* flags;       // [chain][plane|slab][consumer][producer], zeroed by the host
+    alignas(64) CUtensorMap tm_qs[2];  // slab-layout TMA boxes, as in ContourArgs
+    alignas(64) CUtensorMap tm_ws[2];
 };
 
 template <int N, bool EO>
-__global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel_f32(const ContourArgsF a) {
+__global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel_f32(const __grid_constant__ ContourArgsF a) {
     using S = AltShapeF<N, EO>;
     constexpr int LF = S::LF;
     constexpr int OFFY = AxisShapeF<N, EO>::SIZE;
     constexpr int OFFZ = 2 * AxisShapeF<N, EO>::SIZE;
     constexpr int TPR = kContourThreads / N;
     constexpr int CPT = (N / 4 + TPR - 1) / TPR;
+    constexpr unsigned TILE_BYTES = N * N * sizeof(float);
     static_assert(TPR >= 1, "tile rows must not exceed the block");
-    extern __shared__ __align__(16) float smemf[];
+    extern __shared__ __align__(128) unsigned char smemf_raw[];
+    // the dynamic window is only guaranteed 16-byte alignment; TMA tiles need 128
+    float* smemf = reinterpret_cast<float*>(smemf_raw + ((128u - (smem_u32(smemf_raw) & 127u)) & 127u));
     float* sops = smemf;
     float* T0 = smemf + S::OPS_PAD;
     float* T1 = T0 + S::TILE;
-    float* W0 = T1 + S::TILE;
-    float* W1 = W0 + S::TILE;
+    float* WP = T1 + S::TILE;  // [block A, block B] plane-layout factors of this unit
+    float* WS = WP + 2 * S::WT;  // [block A, block B] slab-layout factors
+    float* QS = WS + 2 * S::WT;  // finished q(s+1), drained by bulk stores
+    __shared__ __align__(8) unsigned long long s_bar;
     __shared__ int s_fail;
-    for (int i = threadIdx.x; i < S::OPS; i += kContourThreads) sops[i] = a.ops[i];
-    if (threadIdx.x == 0) s_fail = 0;
 
     constexpr long long M = (long long)N * N * N;
     constexpr long long PLANE = (long long)N * N;
     const int units = a.nchain * N;
+    const int u = blockIdx.x;  // one unit per block: the host launches units <= SMs blocks
+    if (units > (int)gridDim.x) {
+        if (threadIdx.x == 0) atomicOr(a.error, 4);
+        return;
+    }
+    if (u >= units) return;
+    const int warp = threadIdx.x >> 5;
+    const int c = u >= N ? 1 : 0, p = u - c * N;
+    const int dir = c ? a.dir[1] : a.dir[0];
+    const long long slot0 = c ? a.slot0[1] : a.slot0[0];
+    float* q = c ? a.q[1] : a.q[0];
+    float* XP = c ? a.xbuf[1] : a.xbuf[0];
+    float* XS = XP + M;
+    // flags[chain][producing layout][consumer][producer]: every consumer polls its own
+    // N flags (one cache line per 32), written by the producers (push), so the waits of
+    // different blocks never share a line
+    unsigned* fl_plane = a.flags + (size_t)c * 2 * N * N;  // written by plane units
+    unsigned* fl_slab = fl_plane + (size_t)N * N;           // written by slab units
     const int U = a.t_end;
+    {
+        const void* tiles[6] = {WP, WP + S::WT, WS, WS + S::WT, QS, T0};
+        const int e = tma_alignment_error(tiles, 5, a.tm_qs, 2) | tma_alignment_error(tiles, 0, a.tm_ws, 2);
+        if (e) {
+            if (threadIdx.x == 0) atomicOr(a.error, e);
+            return;
+        }
+    }
 
-    auto w_of = [&](int c, int s) -> const float* {
-        const int dir = c ? a.dir[1] : a.dir[0];
-        const long long in_slot = (c ? a.slot0[1] : a.slot0[0]) + (long long)dir * s;
+    if (threadIdx.x == 0) {
+        s_fail = 0;
+        mbar_init(&s_bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (warp == 0) {
+        // the unit's Boltzmann factors of both blocks in both layouts, once per launch
+        if ((threadIdx.x & 31) == 0) mbar_expect_tx(&s_bar, 4 * TILE_BYTES);
+        __syncwarp();
+        for (int b = 0; b < 2; ++b) {
+            bulk_tile_load<float, N>(WP + b * S::WT, a.wds[b], p, true, &a.tm_ws[b], &s_bar);
+            bulk_tile_load<float, N>(WS + b * S::WT, a.wds[b], p, false, &a.tm_ws[b], &s_bar);
+        }
+    }
+    for (int i = threadIdx.x; i < S::OPS; i += kContourThreads) sops[i] = a.ops[i];
+    // block (0: A, 1: B) of the Boltzmann factor of step s
+    auto blk_of = [&](int s) -> int {
+        const long long in_slot = slot0 + (long long)dir * s;
         const long long seg = dir > 0 ? in_slot : in_slot - 1;
-        return seg < a.NsA ? a.wds[0] : a.wds[1];
+        return seg < a.NsA ? 0 : 1;
     };
-    auto fetch_w = [&](int k, int u) {
-        const int c = u >= N ? 1 : 0, p = u - c * N;
+    if (!mbar_wait(&s_bar, 0, a.spin_limit)) {
+        if (threadIdx.x == 0) atomicOr(a.error, 2);
+        return;
+    }
+
+    for (int k = 0; k <= U; ++k) {
         const bool plane = (k & 1) == 0;
         const long long off = plane ? (long long)p * PLANE : (long long)p * N;
         const long long gs = plane ? N : PLANE;
-        if (k >= 1) tile_fetch_f32<N, LF>(W0, w_of(c, k - 1) + off, gs);
-        if (k < U) tile_fetch_f32<N, LF>(W1, w_of(c, k) + off, gs);
-        cp_async_commit();
-    };
-
-    if ((int)blockIdx.x < units) fetch_w(0, blockIdx.x);
-    for (int k = 0; k <= U; ++k) {
-        const bool plane = (k & 1) == 0;
-        for (int u = blockIdx.x; u < units; u += gridDim.x) {
-            const int c = u >= N ? 1 : 0, p = u - c * N;
-            const int dir = c ? a.dir[1] : a.dir[0];
-            const long long slot0 = c ? a.slot0[1] : a.slot0[0];
-            float* q = c ? a.q[1] : a.q[0];
-            float* XP = c ? a.xbuf[1] : a.xbuf[0];
-            float* XS = XP + M;
-            unsigned* fl_plane = a.flags + (size_t)c * 2 * N;
-            unsigned* fl_slab = fl_plane + N;
-            const long long off = plane ? (long long)p * PLANE : (long long)p * N;
-            const long long gs = plane ? N : PLANE;
-            if (u != (int)blockIdx.x) fetch_w(k, u);
-            if (k == 0) {
-                tile_fetch_f32<N, LF>(T0, q + slot0 * M + off, gs);
-            } else {
-                const int r = threadIdx.x / TPR, sub = threadIdx.x - r * TPR;
-                if (r < N) {
-                    const unsigned* f = plane ? fl_slab + r : fl_plane + r;
-                    long long spins = 0;
-                    while (ld_acquire_u32(f) < (unsigned)k) {
-                        if (++spins > a.spin_limit) {
-                            atomicOr(a.error, 1);
-                            s_fail = 1;
-                            break;
-                        }
-                        if (spins > 64) __nanosleep(20);
+        const float* Wl = plane ? WP : WS;
+        if (k == 0) {
+            tile_fetch_f32<N, LF>(T0, q + slot0 * M + off, gs);
+        } else {
+            const int r = threadIdx.x / TPR, sub = threadIdx.x - r * TPR;
+            if (r < N) {
+                const unsigned* f = (plane ? fl_slab : fl_plane) + (size_t)p * N + r;
+                long long spins = 0;
+                while (ld_acquire_u32(f) < (unsigned)k) {
+                    if (++spins > a.spin_limit) {
+                        atomicOr(a.error, 1);
+                        s_fail = 1;
+                        break;
                     }
-                    const float* src = (plane ? XS : XP) + off + r * gs;
+                    if (spins > 64) __nanosleep(20);
+                }
+                const float* src = (plane ? XS : XP) + off + r * gs;
 #pragma unroll
-                    for (int j = 0; j < CPT; ++j) {
-                        const int ch = sub + j * TPR;
-                        if (ch < N / 4) cp_async16(T0 + r * LF + 4 * ch, src + 4 * ch);
-                    }
+                for (int j = 0; j < CPT; ++j) {
+                    const int ch = sub + j * TPR;
+                    if (ch < N / 4) cp_async16(T0 + r * LF + 4 * ch, src + 4 * ch);
                 }
             }
-            cp_async_commit();
-            cp_async_wait_all();
-            __syncthreads();
-            if (s_fail) return;
-            float* cur = T0;
-            float* oth = T1;
-            if (k >= 1) {
-                if (plane) {
-                    row_op_f32<N, N, LF, EO>(cur, oth, sops + OFFZ);
-                    __syncthreads();
-                    col_op_f32<N, N, LF, EO>(oth, cur, sops + OFFY);
-                } else {
-                    col_op_f32<N, N, LF, EO>(cur, oth, sops);
-                    float* tmp = cur;
-                    cur = oth;
-                    oth = tmp;
-                }
+        }
+        cp_async_commit();
+        cp_async_wait_all();
+        __syncthreads();
+        if (s_fail) {
+            if (warp == 0) bulk_wait_all();
+            return;
+        }
+        float* cur = T0;
+        float* oth = T1;
+        if (k >= 1) {
+            if (plane) {
+                row_op_f32<N, N, LF, EO>(cur, oth, sops + OFFZ);
                 __syncthreads();
-                const long long out_slot = slot0 + (long long)dir * k;
-                tile_finish_f32<N, LF>(cur, W0, W1, q + out_slot * M + off, gs, k < U);
+                col_op_f32<N, N, LF, EO>(oth, cur, sops + OFFY);
             } else {
-                tile_scale_f32<N, LF>(cur, W1);
+                col_op_f32<N, N, LF, EO>(cur, oth, sops);
+                float* tmp = cur;
+                cur = oth;
+                oth = tmp;
             }
+            if (warp == 0) bulk_wait_read();  // the previous q store has left QS
             __syncthreads();
-            if (k < U) {
-                if (plane) {
-                    row_op_f32<N, N, LF, EO>(cur, oth, sops + OFFZ);
-                    __syncthreads();
-                    col_op_f32<N, N, LF, EO>(oth, cur, sops + OFFY);
-                } else {
-                    col_op_f32<N, N, LF, EO>(cur, oth, sops);
-                    float* tmp = cur;
-                    cur = oth;
-                    oth = tmp;
-                }
-                __syncthreads();
-                tile_store_f32<N, LF>(cur, (plane ? XP : XS) + off, gs);
-                __syncthreads();
-                if (threadIdx.x == 0) {
-                    __threadfence();
-                    st_release_u32((plane ? fl_plane : fl_slab) + p, (unsigned)(k + 1));
-                }
-            }
+            const float* W0 = Wl + blk_of(k - 1) * S::WT;
+            const float* W1 = Wl + (k < U ? blk_of(k) : 0) * S::WT;
+            tile_finish_f32<N, LF>(cur, W0, W1, QS, k < U);
+            fence_async_smem();
+            __syncthreads();
+            if (warp == 0) bulk_tile_store<float, N>(q, QS, p, slot0 + (long long)dir * k, plane, &a.tm_qs[c]);
+        } else {
+            tile_scale_f32<N, LF>(cur, Wl + blk_of(0) * S::WT);
             __syncthreads();
         }
-        if (k < U && (int)blockIdx.x < units) fetch_w(k + 1, blockIdx.x);
+        if (k < U) {
+            if (plane) {
+                row_op_f32<N, N, LF, EO>(cur, oth, sops + OFFZ);
+                __syncthreads();
+                col_op_f32<N, N, LF, EO>(oth, cur, sops + OFFY);
+            } else {
+                col_op_f32<N, N, LF, EO>(cur, oth, sops);
+                float* tmp = cur;
+                cur = oth;
+                oth = tmp;
+            }
+            __syncthreads();
+            tile_store_f32<N, LF>(cur, (plane ? XP : XS) + off, gs);
+            __syncthreads();
+            if (threadIdx.x < N) {  // tell consumer threadIdx.x that tile p of phase k is out
+                __threadfence();
+                st_release_u32((plane ? fl_plane : fl_slab) + (size_t)threadIdx.x * N + p, (unsigned)(k + 1));
+            }
+        }
+        __syncthreads();
     }
-    cp_async_wait_all();
+    if (warp == 0) bulk_wait_all();
 }
 
 }  // namespace crysscft

@@ -4,6 +4,8 @@
 // (cell, ds) in long double, stored FP64 and FP32 on the device), the
 // triplet/contour launchers, and the AB-diblock iteration context whose whole
 // iteration is captured once into a CUDA graph and replayed.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -47,6 +49,40 @@ int fail(int code, const std::string& msg) {
         int r_ = (call);                   \
         if (r_ != SCFT_OK) return r_;      \
     } while (0)
+
+// TMA descriptor encoder of the driver (cuTensorMapEncodeTiled), resolved once.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// TMA descriptor of the slab-layout tiles of a cubic n^3 field (x, y, z; z fastest): box
+// (z: n, y: 1, x: n) at a fixed y.  slots = 0: one field (rank 3); slots > 0: that many
+// fields back to back, a contour store (rank 4, the slot outermost).
+int encode_slab_map(CUtensorMap* m, const void* base, int n, long long slots, bool fp64) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return fail(SCFT_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    if (reinterpret_cast<uintptr_t>(base) % 16) return fail(SCFT_ERR_INVALID_ARG, "TMA base not 16-byte aligned");
+    const cuuint64_t es = fp64 ? 8 : 4, N = (cuuint64_t)n;
+    cuuint64_t dims[4] = {N, N, N, (cuuint64_t)(slots > 0 ? slots : 1)};
+    cuuint64_t strides[3] = {N * es, N * N * es, N * N * N * es};
+    cuuint32_t box[4] = {(cuuint32_t)n, 1u, (cuuint32_t)n, 1u};
+    cuuint32_t estr[4] = {1u, 1u, 1u, 1u};
+    const CUresult r = enc(m, fp64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                           slots > 0 ? 4u : 3u, const_cast<void*>(base), dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(SCFT_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    return SCFT_OK;
+}
 
 template <typename T>
 struct DevBuf {
@@ -567,11 +603,12 @@ struct scft_diblock_s {
         int per_sm = 0;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, kContourThreads, smem));
         if (per_sm < 1) return SCFT_OK;
+        if (2 * nx > per_sm * sms) return SCFT_OK;  // one unit per block
         contour_fn_f32 = f;
-        persistent_grid = std::min(2 * nx, per_sm * sms);
+        persistent_grid = 2 * nx;
         persistent_smem = smem;
         if (!f_xch.p) CKR(f_xch.alloc(4 * M));
-        if (flags.n != (size_t)(4 * nx)) CKR(flags.alloc((size_t)4 * nx));
+        if (flags.n != (size_t)(4 * nx * nx)) CKR(flags.alloc((size_t)4 * nx * nx));
         if (!ctrl.p) {
             CKR(ctrl.alloc(2));
             CK(cudaMemset(ctrl.p, 0, 2 * sizeof(unsigned)));
@@ -600,6 +637,11 @@ struct scft_diblock_s {
         a.error = reinterpret_cast<int*>(ctrl.p + 1);
         a.spin_limit = spin_limit;
         a.flags = flags.p;
+        const int n = (int)solver->grid_phy[0];
+        CKR(encode_slab_map(&a.tm_qs[0], q, n, (long long)U + 1, false));
+        CKR(encode_slab_map(&a.tm_qs[1], qc, n, (long long)U + 1, false));
+        CKR(encode_slab_map(&a.tm_ws[0], wAds, n, 0, false));
+        CKR(encode_slab_map(&a.tm_ws[1], wBds, n, 0, false));
         CK(cudaMemsetAsync(flags.p, 0, flags.n * sizeof(unsigned), st));
         cudaLaunchConfig_t cfg{};
         cfg.gridDim = dim3((unsigned)persistent_grid);
@@ -646,12 +688,13 @@ struct scft_diblock_s {
             }
         }
         if (!d_xch.p) CKR(d_xch.alloc(4 * M));
-        if (alternating && flags.n != (size_t)(4 * nx)) CKR(flags.alloc((size_t)4 * nx));
+        if (alternating && flags.n != (size_t)(4 * nx * nx)) CKR(flags.alloc((size_t)4 * nx * nx));
         CK(cudaFuncSetAttribute(contour_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 0;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, contour_fn, kContourThreads, smem));
         if (per_sm < 1) return SCFT_OK;
         const int units = 2 * (nx > ny ? nx : ny);
+        if (alternating && units > per_sm * sms) return SCFT_OK;  // one unit per block: per-axis kernels
         persistent_grid = std::min(units, per_sm * sms);
         persistent_smem = smem;
         if (!ctrl.p) {
@@ -693,7 +736,14 @@ struct scft_diblock_s {
         a.spin_limit = spin_limit;
         a.flags = flags.p;
         CK(cudaMemsetAsync(ctrl.p, 0, sizeof(unsigned), st));
-        if (alternating) CK(cudaMemsetAsync(flags.p, 0, flags.n * sizeof(unsigned), st));
+        if (alternating) {
+            const int n = (int)solver->grid_phy[0];
+            CKR(encode_slab_map(&a.tm_qs[0], q, n, (long long)U + 1, true));
+            CKR(encode_slab_map(&a.tm_qs[1], qc, n, (long long)U + 1, true));
+            CKR(encode_slab_map(&a.tm_ws[0], wAds, n, 0, true));
+            CKR(encode_slab_map(&a.tm_ws[1], wBds, n, 0, true));
+            CK(cudaMemsetAsync(flags.p, 0, flags.n * sizeof(unsigned), st));
+        }
         cudaLaunchConfig_t cfg{};
         cfg.gridDim = dim3((unsigned)persistent_grid);
         cfg.blockDim = dim3(kContourThreads);
@@ -1336,7 +1386,10 @@ static int diblock_check_device_error(scft_diblock_t d, cudaStream_t st) {
     if (e) {
         CK(cudaMemsetAsync(d->ctrl.p + 1, 0, sizeof(unsigned), st));
         CK(cudaStreamSynchronize(st));
-        return fail(SCFT_ERR_TIMEOUT, "a grid barrier of the contour kernel gave up waiting");
+        if (e & 24u)
+            return fail(SCFT_ERR_CUDA, "contour kernel: bulk-copy operand misaligned (error bits " + std::to_string(e) + ")");
+        return fail(SCFT_ERR_TIMEOUT, "the contour kernel gave up waiting on a barrier, flag or bulk copy (error bits " +
+                                          std::to_string(e) + ")");
     }
     return SCFT_OK;
 }
