@@ -184,6 +184,25 @@ def run_reference_arm(args):
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
+def accuracy_protocol(run, ref_run, start, n_fp32: int, n_polish: int):
+    """|dF/F| and max |dphi| after n_fp32 FP32 + n_polish FP64 iterations of `run` against
+    n_fp32 + n_polish FP64 iterations of `ref_run`, both from the fields `start`."""
+    import numpy as np
+
+    run.set_fields(start["wA"], start["wB"])
+    run.set_precision("fp32")
+    run.iterate(n_fp32)
+    run.set_precision("fp64")
+    h = run.iterate(n_polish)
+    got = run.get_fields()
+    ref_run.set_fields(start["wA"], start["wB"])
+    hr = ref_run.iterate(n_fp32 + n_polish)
+    want = ref_run.get_fields()
+    return {"dF_over_F": float(abs(h["F"][-1] - hr["F"][-1]) / abs(hr["F"][-1])),
+            "phi_max_abs": float(max(np.abs(got["phiA"] - want["phiA"]).max(),
+                                     np.abs(got["phiB"] - want["phiB"]).max()))}
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -247,7 +266,7 @@ def run_ours(args):
     ms = ev0.elapsed_time(ev1)
     precision_form = None
     if polish:
-        # the same K iterations in plain FP64 from the same fields: |dF/F| of the last one
+        # speed: the same K iterations in plain FP64 from the same fields
         ref_run = scft.DiblockSCFT(solver, WORKLOAD["fA"], WORKLOAD["ds"], WORKLOAD["xN"], WORKLOAD["acc"])
         ref_run.set_fields(start_fields["wA"], start_fields["wB"])
         e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -256,10 +275,16 @@ def run_ours(args):
         e3.record(stream)
         e3.synchronize()
         fp64_ms = e2.elapsed_time(e3)
+        dF_timed = abs(hist["F"][-1] - href["F"][-1]) / abs(href["F"][-1])
+        # accuracy on the precision form's protocol: 90 FP32 iterations and 10 FP64 polish
+        # iterations against 100 FP64 iterations, both from the same fields
+        acc = accuracy_protocol(run, ref_run, start_fields, 90, 10)
         ref_run.close()
-        dF = abs(hist["F"][-1] - href["F"][-1]) / abs(href["F"][-1])
         precision_form = {"fp32_iterations": args.steps - polish, "fp64_polish_iterations": polish,
-                          "dF_over_F": dF, "target": 1e-8, "meets_target": bool(dF <= 1e-8),
+                          "protocol": "90 FP32 + 10 FP64 polish iterations vs 100 FP64 iterations, same start",
+                          "dF_over_F": acc["dF_over_F"], "phi_max_abs": acc["phi_max_abs"],
+                          "target": 1e-8, "meets_target": bool(acc["dF_over_F"] <= 1e-8),
+                          "dF_over_F_timed_run": dF_timed,
                           "fp64_plain_iterations_per_s": world * args.steps / (fp64_ms / 1e3),
                           "speedup_vs_fp64_plain": (fp64_ms / ms)}
         run.set_precision("fp32")

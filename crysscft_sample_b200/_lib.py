@@ -71,6 +71,8 @@ SIGNATURES = {
     "scft_batch_configure": (ctypes.c_int, [_vp, _sz, ctypes.c_int]),
     "scft_batch_autotune": (ctypes.c_int, [_vp, _sz, _szp, ctypes.POINTER(ctypes.c_int), _dp]),
     "scft_diblock_get_precision": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int)]),
+    "scft_diblock_set_mixing": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double]),
+    "scft_diblock_get_residuals": (ctypes.c_int, [_vp, _dp, _sz, _szp]),
 }
 
 _lib = None

@@ -6,6 +6,7 @@
 //  phi     : integrate_phi, trapezoid weights (:348-360), both blocks
 //  energy  : the sums of print_energy (:398-424) and the max incompressibility
 //  update  : calc_new_fields, simple mixing (:362-371)
+//  anderson: Anderson mixing in place of calc_new_fields (no counterpart in the reference)
 //
 // Reductions are deterministic: a fixed grid writes per-block partials, the last
 // block to finish (atomic ticket, no waiting) reduces them in a fixed order.
@@ -18,7 +19,8 @@ constexpr int kRedThreads = 256;
 constexpr int kRedMaxBlocks = 592;  // 4 x 148 SMs
 
 // Layout of the per-iteration record written by energy_kernel (doubles).
-enum { HIST_F = 0, HIST_EH, HIST_E0, HIST_E1, HIST_EK, HIST_MAXINC, HIST_Q, HIST_FLAGS, HIST_STRIDE };
+// HIST_RES: rms of the mixing residual r = (xN phiB + ksi - wA, xN phiA + ksi - wB) over both fields
+enum { HIST_F = 0, HIST_EH, HIST_E0, HIST_E1, HIST_EK, HIST_MAXINC, HIST_Q, HIST_FLAGS, HIST_RES, HIST_STRIDE };
 
 struct IterState {
     double Q;            // partition function of the current iteration
@@ -151,25 +153,30 @@ energy_kernel(const double* __restrict__ wA, const double* __restrict__ wB,
               IterState* st, double* __restrict__ hist, unsigned hist_cap) {
     __shared__ double sh[kRedThreads / 32];
     __shared__ bool last;
-    double e1 = 0.0, eh = 0.0, ek = 0.0, mx = 0.0;
+    double e1 = 0.0, eh = 0.0, ek = 0.0, mx = 0.0, rr = 0.0;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < M;
          i += (long long)gridDim.x * blockDim.x) {
         const double pa = phiA[i], pb = phiB[i];
-        e1 += -wA[i] * pa - wB[i] * pb;
+        const double a = wA[i], b = wB[i], x = ksi[i];
+        e1 += -a * pa - b * pb;
         eh += xN * pa * pb;
         const double temp = 1 - pa - pb;
-        ek += -ksi[i] * temp;
+        ek += -x * temp;
         mx = fmax(mx, fabs(temp));
+        const double ra = xN * pb + x - a, rb = xN * pa + x - b;
+        rr += ra * ra + rb * rb;
     }
     e1 = block_sum(e1, sh);
     eh = block_sum(eh, sh);
     ek = block_sum(ek, sh);
     mx = block_max(mx, sh);
+    rr = block_sum(rr, sh);
     if (threadIdx.x == 0) {
-        partials[4 * blockIdx.x + 0] = e1;
-        partials[4 * blockIdx.x + 1] = eh;
-        partials[4 * blockIdx.x + 2] = ek;
-        partials[4 * blockIdx.x + 3] = mx;
+        partials[5 * blockIdx.x + 0] = e1;
+        partials[5 * blockIdx.x + 1] = eh;
+        partials[5 * blockIdx.x + 2] = ek;
+        partials[5 * blockIdx.x + 3] = mx;
+        partials[5 * blockIdx.x + 4] = rr;
         __threadfence();
         const unsigned t = atomicAdd(&st->ticket_e, 1u);
         last = (t == gridDim.x - 1);
@@ -177,17 +184,19 @@ energy_kernel(const double* __restrict__ wA, const double* __restrict__ wB,
     __syncthreads();
     if (!last) return;
     __threadfence();
-    double r1 = 0.0, rh = 0.0, rk = 0.0, rm = 0.0;
+    double r1 = 0.0, rh = 0.0, rk = 0.0, rm = 0.0, rs = 0.0;
     for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
-        r1 += __ldcg(&partials[4 * i + 0]);
-        rh += __ldcg(&partials[4 * i + 1]);
-        rk += __ldcg(&partials[4 * i + 2]);
-        rm = fmax(rm, __ldcg(&partials[4 * i + 3]));
+        r1 += __ldcg(&partials[5 * i + 0]);
+        rh += __ldcg(&partials[5 * i + 1]);
+        rk += __ldcg(&partials[5 * i + 2]);
+        rm = fmax(rm, __ldcg(&partials[5 * i + 3]));
+        rs += __ldcg(&partials[5 * i + 4]);
     }
     r1 = block_sum(r1, sh);
     rh = block_sum(rh, sh);
     rk = block_sum(rk, sh);
     rm = block_max(rm, sh);
+    rs = block_sum(rs, sh);
     if (threadIdx.x == 0) {
         const double Q = st->Q;
         const double fe_entropic_0 = -log(Q);
@@ -205,6 +214,7 @@ energy_kernel(const double* __restrict__ wA, const double* __restrict__ wB,
         h[HIST_MAXINC] = rm;
         h[HIST_Q] = Q;
         h[HIST_FLAGS] = (double)st->error;
+        h[HIST_RES] = sqrt(rs / (2.0 * (double)M));
         st->ticket_e = 0;
     }
 }
@@ -217,6 +227,170 @@ __global__ void update_kernel(double* __restrict__ wA, double* __restrict__ wB,
          i += (long long)gridDim.x * blockDim.x) {
         wA[i] += acc * (xN * phiB[i] + ksi[i] - wA[i]);
         wB[i] += acc * (xN * phiA[i] + ksi[i] - wB[i]);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->iteration += 1;
+}
+
+// ---------------------------------------------------------------------------
+// Anderson mixing (replaces calc_new_fields when enabled; no counterpart in the
+// reference).  The iterate w = (wA, wB) and residual r = (xN phiB + ksi - wA,
+// xN phiA + ksi - wB) of every iteration go into a ring of history + 1 slots of 2M
+// doubles; gram[a][b] = <r_a, r_b> is kept per ring slot.  With D_j = r_0 - r_j
+// (0 the current iterate, j the j-th previous) the update solves
+// sum_j <D_i, D_j> c_j = <D_i, r_0> and sets
+// w <- w_0 + sum_j c_j (w_j - w_0) + beta (r_0 + sum_j c_j (r_j - r_0)).
+// ---------------------------------------------------------------------------
+constexpr int kAndersonMax = 32;
+
+struct AndersonState {
+    int count;    // previous iterates in the ring (<= history)
+    int head;     // ring slot of the current iterate
+    int k;        // previous iterates this iteration's update uses
+    int restart;  // the last solve was singular: history restarted
+    int slot[kAndersonMax + 1];  // slot[0] current, slot[j] the j-th previous
+    double c[kAndersonMax];
+    double gram[(kAndersonMax + 1) * (kAndersonMax + 1)];
+    unsigned ticket;
+};
+
+// W[head] <- (wA, wB), R[head] <- residual
+__global__ void anderson_record_kernel(const double* __restrict__ wA, const double* __restrict__ wB,
+                                       const double* __restrict__ phiA, const double* __restrict__ phiB,
+                                       const double* __restrict__ ksi, double xN, long long M,
+                                       double* __restrict__ W, double* __restrict__ R, const AndersonState* as) {
+    const long long base = (long long)as->head * 2 * M;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < M;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double a = wA[i], b = wB[i], x = ksi[i];
+        W[base + i] = a;
+        W[base + M + i] = b;
+        R[base + i] = xN * phiB[i] + x - a;
+        R[base + M + i] = xN * phiA[i] + x - b;
+    }
+}
+
+// gram[head][s_j] = gram[s_j][head] = <R[head], R[s_j]>, j = 0..count (deterministic:
+// per-block partials, the last block reduces them in block order)
+__global__ void __launch_bounds__(kRedThreads)
+anderson_dots_kernel(const double* __restrict__ R, long long M, int slots, double* __restrict__ partials,
+                     AndersonState* as) {
+    __shared__ double sh[kRedThreads / 32];
+    __shared__ bool last;
+    const int head = as->head, count = as->count;
+    const long long n2 = 2 * M;
+    const double* r0 = R + (long long)head * n2;
+    for (int j = 0; j <= count; ++j) {
+        const int sj = (head - j + slots) % slots;
+        const double* rj = R + (long long)sj * n2;
+        double d = 0.0;
+        for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n2;
+             i += (long long)gridDim.x * blockDim.x)
+            d += r0[i] * rj[i];
+        d = block_sum(d, sh);
+        if (threadIdx.x == 0) partials[(size_t)blockIdx.x * (kAndersonMax + 1) + j] = d;
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned t = atomicAdd(&as->ticket, 1u);
+        last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    for (int j = 0; j <= count; ++j) {
+        double r = 0.0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
+            r += __ldcg(&partials[(size_t)b * (kAndersonMax + 1) + j]);
+        r = block_sum(r, sh);
+        if (threadIdx.x == 0) {
+            const int sj = (head - j + slots) % slots;
+            as->gram[head * (kAndersonMax + 1) + sj] = r;
+            as->gram[sj * (kAndersonMax + 1) + head] = r;
+        }
+    }
+    if (threadIdx.x == 0) as->ticket = 0;
+}
+
+// One thread: the k x k normal equations by Gaussian elimination with partial pivoting;
+// a pivot below 1e-13 of the largest diagonal entry restarts the history (simple step).
+// Then advances the ring.
+__global__ void anderson_solve_kernel(AndersonState* as, int history) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const int slots = history + 1;
+    const int n = as->head, k = as->count;
+    constexpr int G = kAndersonMax + 1;
+    int s[kAndersonMax + 1];
+    for (int j = 0; j <= k; ++j) s[j] = (n - j + slots) % slots;
+    const double* g = as->gram;
+    double U[kAndersonMax][kAndersonMax], V[kAndersonMax];
+    const double g00 = g[n * G + n];
+    double scale = 0.0;
+    for (int i = 1; i <= k; ++i) {
+        V[i - 1] = g00 - g[n * G + s[i]];
+        for (int j = 1; j <= k; ++j) U[i - 1][j - 1] = g00 - g[n * G + s[j]] - g[s[i] * G + n] + g[s[i] * G + s[j]];
+        scale = fmax(scale, fabs(U[i - 1][i - 1]));
+    }
+    bool singular = false;
+    for (int col = 0; col < k && !singular; ++col) {
+        int piv = col;
+        for (int r = col + 1; r < k; ++r)
+            if (fabs(U[r][col]) > fabs(U[piv][col])) piv = r;
+        if (!(fabs(U[piv][col]) > 1e-13 * scale)) {
+            singular = true;
+            break;
+        }
+        if (piv != col) {
+            for (int j = 0; j < k; ++j) {
+                const double t = U[col][j];
+                U[col][j] = U[piv][j];
+                U[piv][j] = t;
+            }
+            const double t = V[col];
+            V[col] = V[piv];
+            V[piv] = t;
+        }
+        for (int r = col + 1; r < k; ++r) {
+            const double f = U[r][col] / U[col][col];
+            for (int j = col; j < k; ++j) U[r][j] -= f * U[col][j];
+            V[r] -= f * V[col];
+        }
+    }
+    if (!singular) {
+        for (int r = k - 1; r >= 0; --r) {
+            double acc = 0.0;
+            for (int j = r + 1; j < k; ++j) acc += U[r][j] * as->c[j];
+            as->c[r] = (V[r] - acc) / U[r][r];
+        }
+    }
+    as->k = singular ? 0 : k;
+    as->restart = singular ? 1 : 0;
+    for (int j = 0; j <= k; ++j) as->slot[j] = s[j];
+    const int kept = singular ? 0 : k;
+    as->count = kept + 1 < history ? kept + 1 : history;
+    as->head = (n + 1) % slots;
+}
+
+// (wA, wB) <- w_0 + sum_j c_j (w_j - w_0) + beta (r_0 + sum_j c_j (r_j - r_0))
+__global__ void anderson_update_kernel(double* __restrict__ wA, double* __restrict__ wB,
+                                       const double* __restrict__ W, const double* __restrict__ R,
+                                       long long M, const AndersonState* as, double beta, IterState* st) {
+    const int k = as->k;
+    const long long n2 = 2 * M;
+    const double* w0 = W + (long long)as->slot[0] * n2;
+    const double* r0 = R + (long long)as->slot[0] * n2;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n2;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double w = w0[i], r = r0[i];
+        double dw = 0.0, dr = 0.0;
+        for (int j = 1; j <= k; ++j) {
+            const long long o = (long long)as->slot[j] * n2 + i;
+            const double c = as->c[j - 1];
+            dw += c * (W[o] - w);
+            dr += c * (R[o] - r);
+        }
+        const double out = (w + dw) + beta * (r + dr);
+        if (i < M) wA[i] = out;
+        else wB[i - M] = out;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) st->iteration += 1;
 }

@@ -546,6 +546,12 @@ struct scft_diblock_s {
     DevBuf<float> f_wAds, f_wBds, f_q, f_qc, f_t[4];
     DevBuf<IterState> state;
     unsigned hist_cap = 1024;
+    // mixing: history 0 = simple mixing with acc (calc_new_fields); > 0 = Anderson mixing
+    int mix_history = 0;
+    double mix_beta = 0.0;
+    DevBuf<double> and_W, and_R, and_partials;  // ring of (history + 1) x 2M iterates / residuals
+    DevBuf<AndersonState> and_state;
+    std::vector<double> last_residuals;         // rms residual of each iteration of the last run
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
     size_t launches_per_iter = 0;
@@ -798,9 +804,25 @@ struct scft_diblock_s {
         energy_kernel<<<rblocks, kRedThreads, 0, st>>>(wA.p, wB.p, phiA.p, phiB.p, ksi.p, xN, MM,
                                                        partials.p, state.p, hist.p, hist_cap);
         CK(cudaGetLastError());
-        update_kernel<<<blocks, 256, 0, st>>>(wA.p, wB.p, phiA.p, phiB.p, ksi.p, xN, acc, MM, state.p);
-        CK(cudaGetLastError());
-        launches += 4;
+        if (mix_history > 0) {
+            anderson_record_kernel<<<blocks, 256, 0, st>>>(wA.p, wB.p, phiA.p, phiB.p, ksi.p, xN, MM, and_W.p,
+                                                          and_R.p, and_state.p);
+            CK(cudaGetLastError());
+            const int dblocks = (int)std::min<long long>(kRedMaxBlocks, (2 * MM + kRedThreads - 1) / kRedThreads);
+            anderson_dots_kernel<<<dblocks, kRedThreads, 0, st>>>(and_R.p, MM, mix_history + 1, and_partials.p,
+                                                                  and_state.p);
+            CK(cudaGetLastError());
+            anderson_solve_kernel<<<1, 32, 0, st>>>(and_state.p, mix_history);
+            CK(cudaGetLastError());
+            anderson_update_kernel<<<grid_blocks(2 * MM, 256), 256, 0, st>>>(wA.p, wB.p, and_W.p, and_R.p, MM,
+                                                                          and_state.p, mix_beta, state.p);
+            CK(cudaGetLastError());
+            launches += 3 + 4;
+        } else {
+            update_kernel<<<blocks, 256, 0, st>>>(wA.p, wB.p, phiA.p, phiB.p, ksi.p, xN, acc, MM, state.p);
+            CK(cudaGetLastError());
+            launches += 4;
+        }
         launches_per_iter = launches;
         return SCFT_OK;
     }
@@ -1202,7 +1224,7 @@ int scft_diblock_create(scft_solver_t s, double fA, double ds, double xN, double
     const size_t M = s->M;
     CKR(d->wA.alloc(M)); CKR(d->wB.alloc(M)); CKR(d->phiA.alloc(M)); CKR(d->phiB.alloc(M));
     CKR(d->ksi.alloc(M));
-    CKR(d->partials.alloc(4 * kRedMaxBlocks));
+    CKR(d->partials.alloc(5 * kRedMaxBlocks));
     CKR(d->hist.alloc((size_t)d->hist_cap * HIST_STRIDE));
     CKR(d->state.alloc(1));
     CK(cudaMemset(d->state.p, 0, sizeof(IterState)));
@@ -1234,8 +1256,45 @@ int scft_diblock_set_fields(scft_diblock_t d, const double* wA, const double* wB
     cudaStream_t st = d->solver->stream;
     CK(cudaMemcpyAsync(d->wA.p, wA, d->M * sizeof(double), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(d->wB.p, wB, d->M * sizeof(double), cudaMemcpyHostToDevice, st));
+    if (d->and_state.p) CK(cudaMemsetAsync(d->and_state.p, 0, sizeof(AndersonState), st));  // new fields: no history
     CK(cudaStreamSynchronize(st));
     d->fields_set = true;
+    return SCFT_OK;
+}
+
+int scft_diblock_set_mixing(scft_diblock_t d, int history, double beta) {
+    if (!d) return fail(SCFT_ERR_INVALID_ARG, "null handle");
+    if (history < 0 || history > kAndersonMax) return fail(SCFT_ERR_INVALID_ARG, "history must be in 0..32");
+    if (history > 0 && !(beta > 0.0)) return fail(SCFT_ERR_INVALID_ARG, "beta must be > 0");
+    CK(cudaSetDevice(d->solver->device));
+    cudaStream_t st = d->solver->stream;
+    CK(cudaStreamSynchronize(st));
+    if (history > 0) {
+        const size_t ring = (size_t)(history + 1) * 2 * d->M;
+        if (d->and_W.n != ring) {
+            CKR(d->and_W.alloc(ring));
+            CKR(d->and_R.alloc(ring));
+        }
+        if (!d->and_partials.p) CKR(d->and_partials.alloc((size_t)kRedMaxBlocks * (kAndersonMax + 1)));
+        if (!d->and_state.p) CKR(d->and_state.alloc(1));
+        CK(cudaMemsetAsync(d->and_state.p, 0, sizeof(AndersonState), st));
+        CK(cudaStreamSynchronize(st));
+    }
+    if (history != d->mix_history || beta != d->mix_beta) {
+        // the captured iteration graphs (both precisions) embed the mixing kernels
+        d->captured_gen = ~0ULL;
+        d->saved_gen[0] = d->saved_gen[1] = ~0ULL;
+    }
+    d->mix_history = history;
+    d->mix_beta = history > 0 ? beta : 0.0;
+    return SCFT_OK;
+}
+
+int scft_diblock_get_residuals(scft_diblock_t d, double* out, size_t capacity, size_t* count) {
+    if (!d || !count) return fail(SCFT_ERR_INVALID_ARG, "null argument");
+    const size_t n = d->last_residuals.size();
+    *count = n;
+    if (out) std::memcpy(out, d->last_residuals.data(), std::min(n, capacity) * sizeof(double));
     return SCFT_OK;
 }
 
@@ -1400,6 +1459,7 @@ static int diblock_run(scft_diblock_t d, size_t n_iter, double* F, double* parts
     CKR(diblock_prepare(d, true));
     size_t done = 0;
     std::vector<double> h;
+    d->last_residuals.clear();
     while (done < n_iter) {
         const size_t chunk = std::min<size_t>(n_iter - done, d->hist_cap);
         IterState zero{};
@@ -1422,6 +1482,7 @@ static int diblock_run(scft_diblock_t d, size_t n_iter, double* F, double* parts
             }
             if (maxinc) maxinc[done + i] = r[HIST_MAXINC];
             if (Q) Q[done + i] = r[HIST_Q];
+            d->last_residuals.push_back(r[HIST_RES]);
             if (r[HIST_FLAGS] != 0.0) bad = true;
         }
         done += chunk;

@@ -136,6 +136,26 @@ class DiblockSCFT:
         check(_lib.load().scft_diblock_get_precision(self._h, ctypes.byref(v)))
         return {0: "fp64", 1: "fp32"}[v.value]
 
+    def set_mixing(self, kind: str = "simple", history: int = 10, beta: float = 0.5):
+        """Field mixing of the following iterations: "simple" (the reference's
+        calc_new_fields with the acceptance given at construction) or "anderson" (device-side
+        Anderson mixing over the last `history` iterates, mixing parameter `beta`; the history
+        starts empty)."""
+        if kind == "simple":
+            check(_lib.load().scft_diblock_set_mixing(self._h, 0, 0.0))
+        elif kind == "anderson":
+            check(_lib.load().scft_diblock_set_mixing(self._h, int(history), float(beta)))
+        else:
+            raise ValueError(f"unknown mixing {kind!r}")
+
+    def residuals(self) -> np.ndarray:
+        """rms residual sqrt(<r, r> / 2M) of each iteration of the last iterate() call."""
+        n = ctypes.c_size_t()
+        check(_lib.load().scft_diblock_get_residuals(self._h, None, 0, ctypes.byref(n)))
+        out = np.empty(n.value)
+        check(_lib.load().scft_diblock_get_residuals(self._h, _lib.dptr(out), n.value, ctypes.byref(n)))
+        return out
+
     def iterate_polished(self, n_iter: int, n_polish: int):
         """The precision form: n_iter - n_polish FP32 iterations, then n_polish FP64 ones."""
         self.set_precision("fp32")

@@ -189,6 +189,20 @@ int scft_diblock_iterate_host(scft_diblock_t d, double* wA, double* wB, size_t n
 int scft_diblock_set_precision(scft_diblock_t d, int precision);
 int scft_diblock_get_precision(scft_diblock_t d, int* out);
 
+/* Field mixing of the iteration.  history = 0: the reference's simple mixing
+ * w += acceptance (xN phi_other + ksi - w) (calc_new_fields, src/crysSCFT_sample.cpp:362-371;
+ * the default).  history = 1..32: Anderson mixing over the last `history` iterates with
+ * mixing parameter beta > 0, entirely on the device (no counterpart in the reference):
+ * with residual r = (xN phiB + ksi - wA, xN phiA + ksi - wB) and D_j = r_0 - r_j it solves
+ * sum_j <D_i, D_j> c_j = <D_i, r_0> and sets w <- w_0 + sum_j c_j (w_j - w_0)
+ * + beta (r_0 + sum_j c_j (r_j - r_0)); a singular system restarts the history.
+ * The history is cleared by this call and by scft_diblock_set_fields. */
+int scft_diblock_set_mixing(scft_diblock_t d, int history, double beta);
+
+/* rms residual sqrt(<r, r> / 2M) of each iteration of the last scft_diblock_iterate
+ * call (any mixing); *count = number of iterations, at most `capacity` copied. */
+int scft_diblock_get_residuals(scft_diblock_t d, double* out, size_t capacity, size_t* count);
+
 /* Number of kernel launches the last scft_diblock_iterate issued per iteration. */
 int scft_diblock_launches_per_iteration(scft_diblock_t d, size_t* out);
 

@@ -292,6 +292,106 @@ def scft_iterations(solver, fA, ds, xN, L, acceptance, nstep, wA0, wB0):
 
 
 # --------------------------------------------------------------------------
+# Anderson mixing (no counterpart in the reference, which mixes simply,
+# src/crysSCFT_sample.cpp:362-371); restated here as the checker of the
+# library's device-side Anderson mixing.
+# --------------------------------------------------------------------------
+def anderson_step(w_hist, r_hist, beta):
+    """One Anderson-mixing update from the iterates w_hist[0..k] and residuals
+    r_hist[0..k] (index 0 the current iterate, j the j-th previous one; each entry the
+    pair (A field, B field) flattened into one vector).  With D_j = r_0 - r_j it solves
+    sum_j <D_i, D_j> c_j = <D_i, r_0> (i, j = 1..k; <a, b> = a . b) and returns
+    w_bar + beta r_bar, w_bar = w_0 + sum_j c_j (w_j - w_0), r_bar = r_0 + sum_j c_j (r_j - r_0).
+    A singular system (pivot below 1e-13 of the largest diagonal) falls back to the
+    simple step w_0 + beta r_0 and asks for a history restart (second return value)."""
+    k = len(w_hist) - 1
+    r0, w0 = r_hist[0], w_hist[0]
+    if k == 0:
+        return w0 + beta * r0, False
+    G = np.array([[float(np.dot(a, b)) for b in r_hist] for a in r_hist])
+    U = np.empty((k, k))
+    V = np.empty(k)
+    for i in range(1, k + 1):
+        V[i - 1] = G[0, 0] - G[0, i]
+        for j in range(1, k + 1):
+            U[i - 1, j - 1] = G[0, 0] - G[0, j] - G[i, 0] + G[i, j]
+    c = _solve_pivoted(U, V)
+    if c is None:
+        return w0 + beta * r0, True
+    wbar = w0 + sum(c[j - 1] * (w_hist[j] - w0) for j in range(1, k + 1))
+    rbar = r0 + sum(c[j - 1] * (r_hist[j] - r0) for j in range(1, k + 1))
+    return wbar + beta * rbar, False
+
+
+def _solve_pivoted(U, V):
+    """Gaussian elimination with partial pivoting, in the order the device kernel uses;
+    None when a pivot is below 1e-13 of the largest |U_ii|."""
+    U = U.copy()
+    V = V.copy()
+    k = len(V)
+    scale = max(abs(U[i, i]) for i in range(k))
+    for col in range(k):
+        piv = col + int(np.argmax(np.abs(U[col:, col])))
+        if not abs(U[piv, col]) > 1e-13 * scale:
+            return None
+        if piv != col:
+            U[[col, piv]] = U[[piv, col]]
+            V[[col, piv]] = V[[piv, col]]
+        for r in range(col + 1, k):
+            f = U[r, col] / U[col, col]
+            U[r, col:] -= f * U[col, col:]
+            V[r] -= f * V[col]
+    c = np.zeros(k)
+    for r in range(k - 1, -1, -1):
+        c[r] = (V[r] - np.dot(U[r, r + 1:], c[r + 1:])) / U[r, r]
+    return c
+
+
+def scft_iterations_anderson(solver, fA, ds, xN, L, history, beta, nstep, wA0, wB0):
+    """The iteration of scft_iterations with calc_new_fields replaced by Anderson mixing
+    over the last `history` iterates (anderson_step); also returns the rms residual
+    sqrt(<r, r> / (2 M)) of every iteration."""
+    fB = 1 - fA
+    NsA, NsB = contour_counts(fA, ds)
+    shp = solver.grid_phy
+    wA = np.array(wA0, dtype=np.float64).reshape(shp).copy()
+    wB = np.array(wB0, dtype=np.float64).reshape(shp).copy()
+    solver.set_cell_para(L)
+    solver.set_contour_step(ds)
+    hist = {"F": [], "maxinc": [], "Q": [], "residual": []}
+    W, R = [], []
+    phiA = phiB = None
+    for _ in range(nstep):
+        ksi = 0.5 * (wA + wB - xN)
+        wAds = np.exp((-ds / 2) * wA)
+        wBds = np.exp((-ds / 2) * wB)
+        ones = np.ones(shp)
+        qA = solve_diffusion_equation(solver, ones, wAds, NsA, 1)
+        qcB = solve_diffusion_equation(solver, ones, wBds, NsB, -1)
+        qB = solve_diffusion_equation(solver, qA[NsA], wBds, NsB, 1)
+        qcA = solve_diffusion_equation(solver, qcB[0], wAds, NsA, -1)
+        Q = float(np.sum(qcA[0])) / qcA[0].size
+        phiA = integrate_phi(qA, qcA, fA, Q, NsA)
+        phiB = integrate_phi(qB, qcB, fB, Q, NsB)
+        F, parts, mi = energy_terms(Q, xN, wA, wB, phiA, phiB, ksi)
+        r = np.concatenate([(xN * phiB + ksi - wA).ravel(), (xN * phiA + ksi - wB).ravel()])
+        w = np.concatenate([wA.ravel(), wB.ravel()])
+        hist["F"].append(F); hist["maxinc"].append(mi); hist["Q"].append(Q)
+        hist["residual"].append(math.sqrt(float(np.dot(r, r)) / r.size))
+        W.insert(0, w)
+        R.insert(0, r)
+        del W[history + 1:], R[history + 1:]
+        wn, restart = anderson_step(W, R, beta)
+        if restart:
+            del W[1:], R[1:]
+        wA = wn[:wA.size].reshape(shp)
+        wB = wn[wA.size:].reshape(shp)
+    out = {k: np.array(v) for k, v in hist.items()}
+    out.update(phiA=phiA, phiB=phiB, wA=wA, wB=wB)
+    return out
+
+
+# --------------------------------------------------------------------------
 # field-layout conventions of main(), src/crysSCFT_sample.cpp:202-258
 # --------------------------------------------------------------------------
 def extract_3m(full):
