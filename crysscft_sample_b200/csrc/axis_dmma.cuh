@@ -1,0 +1,134 @@
+// Axis passes on the FP64 tensor cores for large cubic grids (n = 96, 128), where the
+// whole-contour kernels do not fit in shared memory: one persistent launch per pass
+// (z, y or x) over both contour chains, the axis operator resident in shared memory
+// (even/odd form when centrosymmetric), DMMA tiles from the contour kernel
+// (row_op_ct / col_op_ct), and the next tile prefetched into registers while the
+// current one is on the tensor cores.  The Boltzmann factor exp(-w ds/2) of the
+// contour step is applied on the z-pass input (pre) and the x-pass output (post),
+// as in the per-axis SIMT kernels (axis_kernels.cuh) these replace for such grids.
+//
+//   z pass: rows of n contiguous values, tile = kRowsZ rows x n      (row_op_ct)
+//   y pass: for one x, tile = n (y) x kColsYX (z) with row stride n   (col_op_ct)
+//   x pass: for one y, tile = n (x) x kColsYX (z) with row stride n^2 (col_op_ct)
+#pragma once
+#include <cuda_runtime.h>
+
+#include "contour_kernel.cuh"
+
+namespace crysscft {
+
+constexpr int kRowsZ = 32;
+constexpr int kColsYX = 32;
+
+struct AxisPassD {
+    const double* in[2];
+    double* out[2];
+    const double* pre[2];   // z pass: input *= pre (nullptr: none)
+    const double* post[2];  // x pass: output *= post (nullptr: none)
+    const double* op;       // this axis' packed operator (AxisShape<N, EO> layout)
+    int nchain;
+};
+
+template <int N, bool EO>
+struct AxisDmmaShape {
+    static constexpr int OPS = (AxisShape<N, EO>::SIZE + 15) & ~15;
+    static constexpr int LFZ = N + 4;       // z tile: kRowsZ x N
+    static constexpr int LFC = kColsYX + 4;  // y/x tile: N x kColsYX
+    static constexpr int TILE = (N * LFC > kRowsZ * LFZ ? N * LFC : kRowsZ * LFZ);
+    static constexpr int TILE_PAD = (TILE + 15) & ~15;
+    static constexpr size_t SMEM = (size_t)(OPS + 2 * TILE_PAD) * sizeof(double);
+    static constexpr int PER_THREAD = N * kColsYX / 2 / kContourThreads;  // double2 per thread and tile
+    static_assert(N * kColsYX == kRowsZ * N, "z and y/x tiles hold the same number of values");
+    static_assert(PER_THREAD * 2 * kContourThreads == N * kColsYX, "tile not a multiple of the block");
+};
+
+// element (r, c) of tile `t` (double2 granularity: c even) and its global offset
+template <int N, int AX>
+struct AxisTiling {
+    static constexpr long long M = (long long)N * N * N;
+    static constexpr int TILES_PER_CHAIN = (AX == 2) ? (N * N / kRowsZ) : (N * (N / kColsYX));
+    // global offset of the tile's origin within its chain and the row stride
+    __device__ static long long origin(int t) {
+        if (AX == 2) return (long long)t * kRowsZ * N;
+        const int a = t / (N / kColsYX), zb = t - a * (N / kColsYX);
+        return AX == 1 ? (long long)a * N * N + zb * kColsYX : (long long)a * N + zb * kColsYX;
+    }
+    static constexpr long long ROW_STRIDE = AX == 2 ? N : (AX == 1 ? N : (long long)N * N);
+    static constexpr int ROW_LEN = AX == 2 ? N : kColsYX;  // values per tile row
+};
+
+template <int N, bool EO, int AX>
+__global__ void __launch_bounds__(kContourThreads, 1) axis_dmma_kernel(const AxisPassD p) {
+    using S = AxisDmmaShape<N, EO>;
+    using TL = AxisTiling<N, AX>;
+    constexpr int LF = AX == 2 ? S::LFZ : S::LFC;
+    constexpr int RL = TL::ROW_LEN;
+    constexpr int PT = S::PER_THREAD;
+    extern __shared__ __align__(16) double axs[];
+    double* sop = axs;
+    double* F = axs + S::OPS;
+    double* G = F + S::TILE_PAD;
+    for (int i = threadIdx.x; i < AxisShape<N, EO>::SIZE; i += kContourThreads) sop[i] = p.op[i];
+
+    const int tiles = p.nchain * TL::TILES_PER_CHAIN;
+    double2 v[PT], w[PT];
+    // fetch tile t into registers (input x pre for the z pass; post for the x pass)
+    auto fetch = [&](int t) {
+        const int c = t / TL::TILES_PER_CHAIN;
+        const long long o = TL::origin(t - c * TL::TILES_PER_CHAIN);
+        const double* in = p.in[c] + o;
+        const double* aux = AX == 2 ? p.pre[c] : (AX == 0 ? p.post[c] : nullptr);
+#pragma unroll
+        for (int k = 0; k < PT; ++k) {
+            const int e = (k * kContourThreads + threadIdx.x) * 2;
+            const int r = e / RL, cc = e - r * RL;
+            const long long g = r * TL::ROW_STRIDE + cc;
+            v[k] = __ldcg(reinterpret_cast<const double2*>(in + g));
+            if (aux) w[k] = __ldg(reinterpret_cast<const double2*>(aux + o + g));
+        }
+    };
+    int t = blockIdx.x;
+    if (t < tiles) fetch(t);
+    for (; t < tiles; t += gridDim.x) {
+        const int c = t / TL::TILES_PER_CHAIN;
+        const long long o = TL::origin(t - c * TL::TILES_PER_CHAIN);
+        const bool pre = AX == 2 && p.pre[c] != nullptr;
+        const bool post = AX == 0 && p.post[c] != nullptr;
+        __syncthreads();  // the previous tile's G has been stored, F may be overwritten
+#pragma unroll
+        for (int k = 0; k < PT; ++k) {
+            const int e = (k * kContourThreads + threadIdx.x) * 2;
+            const int r = e / RL, cc = e - r * RL;
+            double2 x = v[k];
+            if (pre) {
+                x.x *= w[k].x;
+                x.y *= w[k].y;
+            }
+            *reinterpret_cast<double2*>(F + r * LF + cc) = x;
+        }
+        double2 wpost[PT];
+        if (post) {
+#pragma unroll
+            for (int k = 0; k < PT; ++k) wpost[k] = w[k];
+        }
+        __syncthreads();
+        if (t + (int)gridDim.x < tiles) fetch(t + gridDim.x);  // in flight during the MMAs
+        if constexpr (AX == 2) row_op_ct<kRowsZ, N, LF, EO>(F, G, sop);
+        else col_op_ct<N, kColsYX, LF, EO>(F, G, sop);
+        __syncthreads();
+        double* out = p.out[c] + o;
+#pragma unroll
+        for (int k = 0; k < PT; ++k) {
+            const int e = (k * kContourThreads + threadIdx.x) * 2;
+            const int r = e / RL, cc = e - r * RL;
+            double2 y = *reinterpret_cast<const double2*>(G + r * LF + cc);
+            if (post) {
+                y.x *= wpost[k].x;
+                y.y *= wpost[k].y;
+            }
+            __stcg(reinterpret_cast<double2*>(out + r * TL::ROW_STRIDE + cc), y);
+        }
+    }
+}
+
+}  // namespace crysscft

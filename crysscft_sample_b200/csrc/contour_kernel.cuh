@@ -441,9 +441,26 @@ __device__ __forceinline__ void row_op_ct(const double* __restrict__ F, double* 
     }
 }
 
-// G[i][c] = sum_j A[i][j] F[j][c] on an R x C slab (leading dimension LF)
-template <int R, int C, int LF, bool EO>
-__device__ __forceinline__ void col_op_ct(const double* __restrict__ F, double* __restrict__ G,
+// Where col_op_ct writes its result G[i][c]: kToSmem, a shared-memory slab (row stride LF);
+// kToGlobal, the global exchange buffer (row stride gs), straight from the MMA
+// accumulators, so the stores overlap the other warps' tiles.
+enum ColEpilogue { kToSmem = 0, kToGlobal = 1 };
+
+struct ColOut {
+    double* G;
+    long long gs;  // kToGlobal: row stride of G
+};
+
+template <int LF, int EPI>
+__device__ __forceinline__ void col_store(const ColOut& o, int i, int c, double v0, double v1) {
+    if (EPI == kToSmem) *reinterpret_cast<double2*>(o.G + i * LF + c) = make_double2(v0, v1);
+    else *reinterpret_cast<double2*>(o.G + i * o.gs + c) = make_double2(v0, v1);
+}
+
+// G[i][c] = sum_j A[i][j] F[j][c] on an R x C slab (leading dimension LF); EPI selects
+// where the result goes (ColEpilogue)
+template <int R, int C, int LF, bool EO, int EPI = kToSmem>
+__device__ __forceinline__ void col_op_ct(const double* __restrict__ F, const ColOut& out,
                                           const double* __restrict__ opE) {
     using S = AxisShape<R, EO>;
     const double* opO = opE + S::HALF;
@@ -504,15 +521,21 @@ __device__ __forceinline__ void col_op_ct(const double* __restrict__ F, double* 
                 const int i = (mb + a) * 8 + g;
                 const int c = (nb + b) * 8 + 2 * t;
                 if (EO) {
-                    *reinterpret_cast<double2*>(G + i * LF + c) =
-                        make_double2(dP[a][b][0] + dR[a][b][0], dP[a][b][1] + dR[a][b][1]);
-                    *reinterpret_cast<double2*>(G + (R - 1 - i) * LF + c) =
-                        make_double2(dP[a][b][0] - dR[a][b][0], dP[a][b][1] - dR[a][b][1]);
+                    col_store<LF, EPI>(out, i, c, dP[a][b][0] + dR[a][b][0], dP[a][b][1] + dR[a][b][1]);
+                    col_store<LF, EPI>(out, R - 1 - i, c, dP[a][b][0] - dR[a][b][0], dP[a][b][1] - dR[a][b][1]);
                 } else {
-                    *reinterpret_cast<double2*>(G + i * LF + c) = make_double2(dP[a][b][0], dP[a][b][1]);
+                    col_store<LF, EPI>(out, i, c, dP[a][b][0], dP[a][b][1]);
                 }
             }
     }
+}
+
+// col_op_ct into a shared-memory slab G
+template <int R, int C, int LF, bool EO>
+__device__ __forceinline__ void col_op_ct(const double* __restrict__ F, double* __restrict__ G,
+                                          const double* __restrict__ opE) {
+    const ColOut o{G, 0};
+    col_op_ct<R, C, LF, EO, kToSmem>(F, o, opE);
 }
 
 // R x C slab between global (row stride gs) and shared memory (row stride LF), optional factor w
@@ -701,18 +724,6 @@ __device__ __forceinline__ void tile_fetch(double* sm, const double* gm, long lo
     for (int e = threadIdx.x; e < TOTAL; e += kContourThreads) {
         const int r = e / PER_ROW, c = (e - r * PER_ROW) * 2;
         cp_async16(sm + r * LF + c, gm + r * gs + c);
-    }
-}
-
-// shared -> global copy of an N x N tile (row stride gs)
-template <int N, int LF>
-__device__ __forceinline__ void tile_store(const double* sm, double* gm, long long gs) {
-    constexpr int PER_ROW = N / 2;
-    constexpr int TOTAL = N * PER_ROW;
-#pragma unroll 4
-    for (int e = threadIdx.x; e < TOTAL; e += kContourThreads) {
-        const int r = e / PER_ROW, c = (e - r * PER_ROW) * 2;
-        *reinterpret_cast<double2*>(gm + r * gs + c) = *reinterpret_cast<const double2*>(sm + r * LF + c);
     }
 }
 
@@ -932,7 +943,7 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
         double* cur = T0;
         double* oth = T1;
         if (k >= 1) {
-            // finish step k-1: the axis ops this layout owns, then D, store q
+            // finish step k-1: the axis ops this layout owns, then D, q(s+1) to the staging tile
             if (plane) {
                 row_op_ct<N, N, LF, EO>(cur, oth, sops + OFFZ);
                 __syncthreads();
@@ -954,6 +965,8 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
         }
         __syncthreads();
         if (k >= 1) {
+            // a separate pass: the dense TMA tiles (row stride n) would bank-conflict with the
+            // MMA fragment pattern of an epilogue
             tile_finish<N, LF>(cur, W0, W1, QS, k < U);
             fence_async_smem();
             __syncthreads();
@@ -964,19 +977,16 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
         }
         if (k < U) {
             if (warp == 0) issue_w(k + 1);  // W0/W1 are free: prefetch the next phase's factors
-            // start step k on this layout; the other layout finishes it next phase
+            // start step k on this layout; the last op's epilogue writes the exchange buffer,
+            // which the other layout finishes next phase
+            const ColOut xo{(plane ? XP : XS) + off, gs};
             if (plane) {
                 row_op_ct<N, N, LF, EO>(cur, oth, sops + OFFZ);
                 __syncthreads();
-                col_op_ct<N, N, LF, EO>(oth, cur, sops + OFFY);
+                col_op_ct<N, N, LF, EO, kToGlobal>(oth, xo, sops + OFFY);
             } else {
-                col_op_ct<N, N, LF, EO>(cur, oth, sops);
-                double* tmp = cur;
-                cur = oth;
-                oth = tmp;
+                col_op_ct<N, N, LF, EO, kToGlobal>(cur, xo, sops);
             }
-            __syncthreads();
-            tile_store<N, LF>(cur, (plane ? XP : XS) + off, gs);
             __syncthreads();
             if (threadIdx.x < N) {  // tell consumer threadIdx.x that tile p of phase k is out
                 __threadfence();

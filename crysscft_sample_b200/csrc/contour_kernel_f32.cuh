@@ -163,9 +163,22 @@ __device__ __forceinline__ void row_op_f32(const float* __restrict__ F, float* _
     }
 }
 
+// Destination of col_op_f32 (ColEpilogue of the FP64 kernel): a shared slab or the global
+// exchange buffer.
+struct ColOutF {
+    float* G;
+    long long gs;
+};
+
+template <int LF, int EPI>
+__device__ __forceinline__ void col_store_f32(const ColOutF& o, int i, int c, float v0, float v1) {
+    if (EPI == kToSmem) *reinterpret_cast<float2*>(o.G + i * LF + c) = make_float2(v0, v1);
+    else *reinterpret_cast<float2*>(o.G + i * o.gs + c) = make_float2(v0, v1);
+}
+
 // G[i][c] = sum_j A[i][j] F[j][c] on an R x C slab: m16 tiles over i, n8 tiles over c
-template <int R, int C, int LF, bool EO>
-__device__ __forceinline__ void col_op_f32(const float* __restrict__ F, float* __restrict__ G,
+template <int R, int C, int LF, bool EO, int EPI = kToSmem>
+__device__ __forceinline__ void col_op_f32(const float* __restrict__ F, const ColOutF& out,
                                            const float* __restrict__ op) {
     using S = AxisShapeF<R, EO>;
     constexpr int MI = S::K, K = S::K, LD = S::LD;
@@ -230,17 +243,25 @@ __device__ __forceinline__ void col_op_f32(const float* __restrict__ F, float* _
                 const float p0 = dP[b][2 * h], p1 = dP[b][2 * h + 1];
                 if (EO) {
                     const float r0 = dR[b][2 * h], r1 = dR[b][2 * h + 1];
-                    *reinterpret_cast<float2*>(G + i * LF + c) = make_float2(p0 + r0, p1 + r1);
-                    *reinterpret_cast<float2*>(G + (R - 1 - i) * LF + c) = make_float2(p0 - r0, p1 - r1);
+                    col_store_f32<LF, EPI>(out, i, c, p0 + r0, p1 + r1);
+                    col_store_f32<LF, EPI>(out, R - 1 - i, c, p0 - r0, p1 - r1);
                 } else {
-                    *reinterpret_cast<float2*>(G + i * LF + c) = make_float2(p0, p1);
+                    col_store_f32<LF, EPI>(out, i, c, p0, p1);
                 }
             }
         }
     }
 }
 
-// ---- N x N FP32 tiles between global (row stride gs) and shared memory (row stride LF)
+// col_op_f32 into a shared-memory slab G
+template <int R, int C, int LF, bool EO>
+__device__ __forceinline__ void col_op_f32(const float* __restrict__ F, float* __restrict__ G,
+                                           const float* __restrict__ op) {
+    const ColOutF o{G, 0};
+    col_op_f32<R, C, LF, EO, kToSmem>(F, o, op);
+}
+
+// N x N FP32 tile from global (row stride gs) into shared memory (row stride LF) with cp.async
 template <int N, int LF>
 __device__ __forceinline__ void tile_fetch_f32(float* sm, const float* gm, long long gs) {
     constexpr int PER_ROW = N / 4;
@@ -251,16 +272,7 @@ __device__ __forceinline__ void tile_fetch_f32(float* sm, const float* gm, long 
         cp_async16(sm + r * LF + c, gm + r * gs + c);
     }
 }
-template <int N, int LF>
-__device__ __forceinline__ void tile_store_f32(const float* sm, float* gm, long long gs) {
-    constexpr int PER_ROW = N / 4;
-    constexpr int TOTAL = N * PER_ROW;
-#pragma unroll 4
-    for (int e = threadIdx.x; e < TOTAL; e += kContourThreads) {
-        const int r = e / PER_ROW, c = (e - r * PER_ROW) * 4;
-        *reinterpret_cast<float4*>(gm + r * gs + c) = *reinterpret_cast<const float4*>(sm + r * LF + c);
-    }
-}
+
 // T <- T * W (T row stride LF, W dense N x N)
 template <int N, int LF>
 __device__ __forceinline__ void tile_scale_f32(float* T, const float* W) {
@@ -466,6 +478,8 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel_f32(con
             }
             if (warp == 0) bulk_wait_read();  // the previous q store has left QS
             __syncthreads();
+            // a separate pass: the dense TMA tiles (row stride n) would bank-conflict with the
+            // MMA fragment pattern of an epilogue
             const float* W0 = Wl + blk_of(k - 1) * S::WT;
             const float* W1 = Wl + (k < U ? blk_of(k) : 0) * S::WT;
             tile_finish_f32<N, LF>(cur, W0, W1, QS, k < U);
@@ -477,18 +491,15 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel_f32(con
             __syncthreads();
         }
         if (k < U) {
+            // start step k; the last op's epilogue writes the exchange buffer
+            const ColOutF xo{(plane ? XP : XS) + off, gs};
             if (plane) {
                 row_op_f32<N, N, LF, EO>(cur, oth, sops + OFFZ);
                 __syncthreads();
-                col_op_f32<N, N, LF, EO>(oth, cur, sops + OFFY);
+                col_op_f32<N, N, LF, EO, kToGlobal>(oth, xo, sops + OFFY);
             } else {
-                col_op_f32<N, N, LF, EO>(cur, oth, sops);
-                float* tmp = cur;
-                cur = oth;
-                oth = tmp;
+                col_op_f32<N, N, LF, EO, kToGlobal>(cur, xo, sops);
             }
-            __syncthreads();
-            tile_store_f32<N, LF>(cur, (plane ? XP : XS) + off, gs);
             __syncthreads();
             if (threadIdx.x < N) {  // tell consumer threadIdx.x that tile p of phase k is out
                 __threadfence();

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/crysscft_b200.h"
+#include "axis_dmma.cuh"
 #include "axis_kernels.cuh"
 #include "contour_kernel.cuh"
 #include "contour_kernel_f32.cuh"
@@ -279,6 +280,26 @@ cudaError_t launch_axis(const AxisPass<T>& p, int nchain, bool contiguous, cudaS
     return launch_strided_bm<T, 64>(p, nchain, st);
 }
 
+using AxisDmmaFn = void (*)(const AxisPassD);
+
+// The FP64 tensor-core axis pass for a cubic grid of side n (96 or 128); nullptr if none.
+AxisDmmaFn axis_dmma_kernel_for(int n, int eo, int ax, size_t* smem) {
+#define CRYSSCFT_AXD(N, E)                                            \
+    {                                                                 \
+        *smem = AxisDmmaShape<N, E>::SMEM;                            \
+        return ax == 0 ? axis_dmma_kernel<N, E, 0>                    \
+                       : (ax == 1 ? axis_dmma_kernel<N, E, 1> : axis_dmma_kernel<N, E, 2>); \
+    }
+    if (n == 128) {
+        if (eo) CRYSSCFT_AXD(128, true) else CRYSSCFT_AXD(128, false)
+    }
+    if (n == 96) {
+        if (eo) CRYSSCFT_AXD(96, true) else CRYSSCFT_AXD(96, false)
+    }
+#undef CRYSSCFT_AXD
+    return nullptr;
+}
+
 using ContourFn = void (*)(const ContourArgs);
 
 // The alternating-layout contour kernel for cubic grids whose four tiles and operators
@@ -379,6 +400,9 @@ struct scft_solver_s {
     int kind = 0;
     int precision = SCFT_FP64;
     int device = 0;
+    int sms = 0;                   // multiprocessors of `device` (queried on first use)
+    size_t axis_dmma_smem_set = 0; // dynamic shared memory granted to the tensor-core axis passes
+    bool force_simt_axes = false;  // tests: run the SIMT per-axis kernels even where DMMA passes exist
     size_t grid_log[3] = {0, 0, 0};
     size_t grid_phy[3] = {0, 0, 0};
     size_t M = 0;
@@ -502,6 +526,41 @@ struct scft_solver_s {
         for (int c = 0; c < nchain && nt > 1; ++c)
             if ((const void*)io[c].in == (const void*)io[c].out)
                 return fail(SCFT_ERR_INVALID_ARG, "multi-term triplet: input and output alias");
+        if constexpr (sizeof(T) == 8) {
+            // large cubic grids: the three passes on the FP64 tensor cores (axis_dmma.cuh)
+            if (nt == 1 && nx == ny && ny == nz && ops->eo[0] == ops->eo[1] && ops->eo[1] == ops->eo[2] &&
+                !force_simt_axes) {
+                AxisDmmaFn f[3];
+                size_t smem = 0;
+                for (int ax = 0; ax < 3; ++ax) f[ax] = axis_dmma_kernel_for(nx, ops->eo[ax], ax, &smem);
+                if (f[0] && f[1] && f[2]) {
+                    if (!sms) CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+                    if (axis_dmma_smem_set != smem) {
+                        for (int ax = 0; ax < 3; ++ax)
+                            CK(cudaFuncSetAttribute(f[ax], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                        axis_dmma_smem_set = smem;
+                    }
+                    AxisPassD pz{}, py{}, px{};
+                    for (int c = 0; c < nchain; ++c) {
+                        pz.in[c] = io[c].in; pz.out[c] = t1[c]; pz.pre[c] = io[c].pre;
+                        py.in[c] = t1[c]; py.out[c] = t2[c];
+                        px.in[c] = t2[c]; px.out[c] = io[c].out; px.post[c] = io[c].post;
+                    }
+                    pz.nchain = py.nchain = px.nchain = nchain;
+                    pz.op = ops->d_packed.p + ops->off[2];
+                    py.op = ops->d_packed.p + ops->off[1];
+                    px.op = ops->d_packed.p + ops->off[0];
+                    f[2]<<<sms, kContourThreads, smem, st>>>(pz);
+                    CK(cudaGetLastError());
+                    f[1]<<<sms, kContourThreads, smem, st>>>(py);
+                    CK(cudaGetLastError());
+                    f[0]<<<sms, kContourThreads, smem, st>>>(px);
+                    CK(cudaGetLastError());
+                    launches += 3;
+                    return SCFT_OK;
+                }
+            }
+        }
         for (int t = 0; t < nt; ++t) {
             OpsSet* o = ops->term(t);
             const T* opx;

@@ -57,6 +57,23 @@ def test_iterations_match_reference_sizes(gpu, kind, N, nstep):
     _compare(want, got)
 
 
+# the FP64 tensor-core axis passes of large cubic grids (128^3 physical: PMMM and 3M on a
+# 256^3 full grid, P1 on 128^3; 96^3 physical: PMMM on 192^3), on a shorter contour
+LARGE = [
+    ("PMMM", (256, 256, 256)),
+    ("3M", (256, 256, 256)),
+    ("P1", (128, 128, 128)),
+    ("PMMM", (192, 192, 192)),
+]
+
+
+@pytest.mark.parametrize("kind,N", LARGE)
+def test_iterations_match_reference_large(gpu, kind, N):
+    cfg = dict(CFG0, N=N, ds=0.02)
+    want, got = _run_pair(kind, cfg, 2)
+    _compare(want, got)
+
+
 def _compare(want, got):
     assert np.all(np.abs(got["F"] - want["F"]) <= F_RTOL * np.abs(want["F"]))
     assert np.abs(got["maxinc"] - want["maxinc"]).max() < 1e-11
