@@ -1,4 +1,4 @@
-// Axis passes on the FP64 tensor cores for large cubic grids (n = 96, 128), where the
+// Axis passes on the tensor cores for large cubic grids (n = 96, 128), where the
 // whole-contour kernels do not fit in shared memory: one persistent launch per pass
 // (z, y or x) over both contour chains, the axis operator resident in shared memory
 // (even/odd form when centrosymmetric), DMMA tiles from the contour kernel
@@ -10,10 +10,13 @@
 //   z pass: rows of n contiguous values, tile = kRowsZ rows x n      (row_op_ct)
 //   y pass: for one x, tile = n (y) x kColsYX (z) with row stride n   (col_op_ct)
 //   x pass: for one y, tile = n (x) x kColsYX (z) with row stride n^2 (col_op_ct)
+// FP64 runs on DMMA (axis_dmma_kernel); the FP32 precision form on 3xTF32 split products
+// (axis_tf32_kernel, row_op_f32 / col_op_f32).
 #pragma once
 #include <cuda_runtime.h>
 
 #include "contour_kernel.cuh"
+#include "contour_kernel_f32.cuh"
 
 namespace crysscft {
 
@@ -127,6 +130,105 @@ __global__ void __launch_bounds__(kContourThreads, 1) axis_dmma_kernel(const Axi
                 y.y *= wpost[k].y;
             }
             __stcg(reinterpret_cast<double2*>(out + r * TL::ROW_STRIDE + cc), y);
+        }
+    }
+}
+
+// ---- FP32 (3xTF32) form ---------------------------------------------------------
+struct AxisPassF {
+    const float* in[2];
+    float* out[2];
+    const float* pre[2];
+    const float* post[2];
+    const float* op;  // this axis' packed TF32 hi/lo operator (AxisShapeF<N, EO> layout)
+    int nchain;
+};
+
+template <int N, bool EO>
+struct AxisTf32Shape {
+    static constexpr int OPS = (AxisShapeF<N, EO>::SIZE + 31) & ~31;
+    static constexpr int LFZ = N + 4;
+    static constexpr int LFC = kColsYX + 4;
+    static constexpr int TILE = (N * LFC > kRowsZ * LFZ ? N * LFC : kRowsZ * LFZ);
+    static constexpr int TILE_PAD = (TILE + 31) & ~31;
+    static constexpr size_t SMEM = (size_t)(OPS + 2 * TILE_PAD) * sizeof(float);
+    static constexpr int PER_THREAD = N * kColsYX / 4 / kContourThreads;  // float4 per thread and tile
+    static_assert(PER_THREAD * 4 * kContourThreads == N * kColsYX, "tile not a multiple of the block");
+};
+
+template <int N, bool EO, int AX>
+__global__ void __launch_bounds__(kContourThreads) axis_tf32_kernel(const AxisPassF p) {
+    using S = AxisTf32Shape<N, EO>;
+    using TL = AxisTiling<N, AX>;
+    constexpr int LF = AX == 2 ? S::LFZ : S::LFC;
+    constexpr int RL = TL::ROW_LEN;
+    constexpr int PT = S::PER_THREAD;
+    extern __shared__ __align__(16) float axf[];
+    float* sop = axf;
+    float* F = axf + S::OPS;
+    float* G = F + S::TILE_PAD;
+    for (int i = threadIdx.x; i < AxisShapeF<N, EO>::SIZE; i += kContourThreads) sop[i] = p.op[i];
+
+    const int tiles = p.nchain * TL::TILES_PER_CHAIN;
+    float4 v[PT], w[PT];
+    auto fetch = [&](int t) {
+        const int c = t / TL::TILES_PER_CHAIN;
+        const long long o = TL::origin(t - c * TL::TILES_PER_CHAIN);
+        const float* in = p.in[c] + o;
+        const float* aux = AX == 2 ? p.pre[c] : (AX == 0 ? p.post[c] : nullptr);
+#pragma unroll
+        for (int k = 0; k < PT; ++k) {
+            const int e = (k * kContourThreads + threadIdx.x) * 4;
+            const int r = e / RL, cc = e - r * RL;
+            const long long g = r * TL::ROW_STRIDE + cc;
+            v[k] = __ldcg(reinterpret_cast<const float4*>(in + g));
+            if (aux) w[k] = __ldg(reinterpret_cast<const float4*>(aux + o + g));
+        }
+    };
+    int t = blockIdx.x;
+    if (t < tiles) fetch(t);
+    for (; t < tiles; t += gridDim.x) {
+        const int c = t / TL::TILES_PER_CHAIN;
+        const long long o = TL::origin(t - c * TL::TILES_PER_CHAIN);
+        const bool pre = AX == 2 && p.pre[c] != nullptr;
+        const bool post = AX == 0 && p.post[c] != nullptr;
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < PT; ++k) {
+            const int e = (k * kContourThreads + threadIdx.x) * 4;
+            const int r = e / RL, cc = e - r * RL;
+            float4 x = v[k];
+            if (pre) {
+                x.x *= w[k].x;
+                x.y *= w[k].y;
+                x.z *= w[k].z;
+                x.w *= w[k].w;
+            }
+            *reinterpret_cast<float4*>(F + r * LF + cc) = x;
+        }
+        float4 wpost[PT];
+        if (post) {
+#pragma unroll
+            for (int k = 0; k < PT; ++k) wpost[k] = w[k];
+        }
+        __syncthreads();
+        if (t + (int)gridDim.x < tiles) fetch(t + gridDim.x);
+        if constexpr (AX == 2) row_op_f32<kRowsZ, N, LF, EO>(F, G, sop);
+        else col_op_f32<N, kColsYX, LF, EO>(F, G, sop);
+        __syncthreads();
+        float* out = p.out[c] + o;
+#pragma unroll
+        for (int k = 0; k < PT; ++k) {
+            const int e = (k * kContourThreads + threadIdx.x) * 4;
+            const int r = e / RL, cc = e - r * RL;
+            float4 y = *reinterpret_cast<const float4*>(G + r * LF + cc);
+            if (post) {
+                y.x *= wpost[k].x;
+                y.y *= wpost[k].y;
+                y.z *= wpost[k].z;
+                y.w *= wpost[k].w;
+            }
+            __stcg(reinterpret_cast<float4*>(out + r * TL::ROW_STRIDE + cc), y);
         }
     }
 }

@@ -300,6 +300,28 @@ AxisDmmaFn axis_dmma_kernel_for(int n, int eo, int ax, size_t* smem) {
     return nullptr;
 }
 
+using AxisTf32Fn = void (*)(const AxisPassF);
+
+// The FP32 (3xTF32) axis pass for a cubic grid of side n (96 or 128); nullptr if none.
+// *op_stride: floats between consecutive axes' operators in the packed FP32 buffer.
+AxisTf32Fn axis_tf32_kernel_for(int n, int eo, int ax, size_t* smem, size_t* op_stride) {
+#define CRYSSCFT_AXF(N, E)                                                                    \
+    {                                                                                         \
+        *smem = AxisTf32Shape<N, E>::SMEM;                                                    \
+        *op_stride = AxisShapeF<N, E>::SIZE;                                                  \
+        return ax == 0 ? axis_tf32_kernel<N, E, 0>                                            \
+                       : (ax == 1 ? axis_tf32_kernel<N, E, 1> : axis_tf32_kernel<N, E, 2>);   \
+    }
+    if (n == 128) {
+        if (eo) CRYSSCFT_AXF(128, true) else CRYSSCFT_AXF(128, false)
+    }
+    if (n == 96) {
+        if (eo) CRYSSCFT_AXF(96, true) else CRYSSCFT_AXF(96, false)
+    }
+#undef CRYSSCFT_AXF
+    return nullptr;
+}
+
 using ContourFn = void (*)(const ContourArgs);
 
 // The alternating-layout contour kernel for cubic grids whose four tiles and operators
@@ -402,6 +424,7 @@ struct scft_solver_s {
     int device = 0;
     int sms = 0;                   // multiprocessors of `device` (queried on first use)
     size_t axis_dmma_smem_set = 0; // dynamic shared memory granted to the tensor-core axis passes
+    size_t axis_tf32_smem_set = 0;
     bool force_simt_axes = false;  // tests: run the SIMT per-axis kernels even where DMMA passes exist
     size_t grid_log[3] = {0, 0, 0};
     size_t grid_phy[3] = {0, 0, 0};
@@ -555,6 +578,44 @@ struct scft_solver_s {
                     f[1]<<<sms, kContourThreads, smem, st>>>(py);
                     CK(cudaGetLastError());
                     f[0]<<<sms, kContourThreads, smem, st>>>(px);
+                    CK(cudaGetLastError());
+                    launches += 3;
+                    return SCFT_OK;
+                }
+            }
+        } else {
+            // large cubic grids, FP32 precision form: 3xTF32 axis passes
+            if (nt == 1 && nx == ny && ny == nz && ops->eo_f32[0] == ops->eo_f32[1] &&
+                ops->eo_f32[1] == ops->eo_f32[2] && !force_simt_axes) {
+                AxisTf32Fn f[3];
+                size_t smem = 0, stride = 0;
+                for (int ax = 0; ax < 3; ++ax) f[ax] = axis_tf32_kernel_for(nx, ops->eo_f32[ax], ax, &smem, &stride);
+                if (f[0] && f[1] && f[2]) {
+                    if (!sms) CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+                    if (axis_tf32_smem_set != smem) {
+                        for (int ax = 0; ax < 3; ++ax)
+                            CK(cudaFuncSetAttribute(f[ax], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                        axis_tf32_smem_set = smem;
+                    }
+                    int per_sm = 1;
+                    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f[2], kContourThreads, smem));
+                    const int grid = sms * (per_sm > 0 ? per_sm : 1);
+                    AxisPassF pz{}, py{}, px{};
+                    for (int c = 0; c < nchain; ++c) {
+                        pz.in[c] = (const float*)io[c].in; pz.out[c] = (float*)t1[c]; pz.pre[c] = (const float*)io[c].pre;
+                        py.in[c] = (const float*)t1[c]; py.out[c] = (float*)t2[c];
+                        px.in[c] = (const float*)t2[c]; px.out[c] = (float*)io[c].out;
+                        px.post[c] = (const float*)io[c].post;
+                    }
+                    pz.nchain = py.nchain = px.nchain = nchain;
+                    pz.op = ops->f_packed.p + 2 * stride;
+                    py.op = ops->f_packed.p + stride;
+                    px.op = ops->f_packed.p;
+                    f[2]<<<grid, kContourThreads, smem, st>>>(pz);
+                    CK(cudaGetLastError());
+                    f[1]<<<grid, kContourThreads, smem, st>>>(py);
+                    CK(cudaGetLastError());
+                    f[0]<<<grid, kContourThreads, smem, st>>>(px);
                     CK(cudaGetLastError());
                     launches += 3;
                     return SCFT_OK;

@@ -36,6 +36,16 @@ def test_fp32_triplets_track_fp64(gpu, kind, N):
     assert rel[:-1].max() > 1e-12             # the FP32 path really ran in FP32
 
 
+@pytest.mark.parametrize("kind,N", [("PMMM", (256, 256, 256)), ("P1", (128, 128, 128))])
+def test_fp32_large_grid_axis_passes_track_fp64(gpu, kind, N):
+    # 128^3 physical: the FP32 triplets run as 3xTF32 tensor-core axis passes
+    want, got = _pair(kind, N, 3, 1, ds=0.02)
+    rel = np.abs(got["F"] - want["F"]) / np.abs(want["F"])
+    assert rel[:-1].max() < FP32_REL
+    assert rel[-1] < rel[:-1].max() / 10
+    assert rel[:-1].max() > 1e-12
+
+
 @pytest.mark.parametrize("kind", ["PMMM", "P1"])
 def test_fp32_plus_polish_reaches_target(gpu, kind):
     want, got = _pair(kind, (32, 32, 32), 40, 2)
