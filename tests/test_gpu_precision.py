@@ -66,3 +66,24 @@ def test_precision_switch_round_trip(gpu):
     assert np.all(np.isfinite(h["F"]))
     run.set_precision("fp64")
     assert np.all(np.isfinite(run.iterate(1)["F"]))
+
+
+def test_switching_precision_back_and_forth_replays_saved_graphs(gpu):
+    # each precision keeps its captured iteration graph; buffers those graphs use must
+    # survive the other precision's setup (FP32 -> FP64 -> FP32 replays the FP32 graph)
+    def sequence():
+        N, L = (64, 64, 64), 4.2
+        wA, wB = fields.seed_fields(N, L, "BCC")
+        G = solvers.make_solver("PMMM", N)
+        G.set_cell_para((L, L, L))
+        run = scft.DiblockSCFT(G, 0.25, 0.01, 20.0, 0.1)
+        run.set_fields(fields.to_physical("PMMM", wA), fields.to_physical("PMMM", wB))
+        out = []
+        for precision, n in (("fp32", 2), ("fp64", 1), ("fp32", 2), ("fp64", 1)):
+            run.set_precision(precision)
+            out.append(run.iterate(n)["F"])
+        return np.concatenate(out)
+
+    a, b = sequence(), sequence()
+    assert np.all(np.isfinite(a))
+    assert np.array_equal(a, b)
