@@ -675,6 +675,10 @@ __device__ __forceinline__ bool mbar_test(unsigned long long* bar, unsigned pari
     return ok != 0;
 }
 // Wait for the phase of `bar` with the given parity to complete; false after `limit` polls.
+// Polls allowed for draining this block's own bulk copies on an error exit, independent
+// of the caller's wait limit (a copy from valid memory completes in microseconds).
+constexpr long long kDrainSpins = 1LL << 24;
+
 __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, long long limit) {
     long long spins = 0;
     while (!mbar_test(bar, parity)) {
@@ -899,7 +903,7 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
     unsigned wpar = 0;  // parity of the pending W phase of s_bar
     // error exit: let this block's bulk copies finish (bounded), then return
     auto drain = [&](bool w_pending) {
-        if (w_pending) mbar_wait(&s_bar, wpar, a.spin_limit);
+        if (w_pending) mbar_wait(&s_bar, wpar, kDrainSpins);
         if (warp == 0) bulk_wait_all();
     };
 
@@ -956,14 +960,14 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
             }
             if (warp == 0) bulk_wait_read();  // the previous q store has left QS
         }
-        const bool w_ok = mbar_wait(&s_bar, wpar, a.spin_limit);
-        wpar ^= 1u;
-        if (!w_ok) {
+        if (!mbar_wait(&s_bar, wpar, a.spin_limit)) s_fail = 1;
+        __syncthreads();
+        if (s_fail) {  // every thread leaves here: the W load still lands in this block's memory first
             if (threadIdx.x == 0) atomicOr(a.error, 2);
-            if (warp == 0) bulk_wait_all();
+            drain(true);
             return;
         }
-        __syncthreads();
+        wpar ^= 1u;
         if (k >= 1) {
             // a separate pass: the dense TMA tiles (row stride n) would bank-conflict with the
             // MMA fragment pattern of an epilogue

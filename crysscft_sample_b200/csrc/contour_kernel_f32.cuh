@@ -423,8 +423,13 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel_f32(con
         const long long seg = dir > 0 ? in_slot : in_slot - 1;
         return seg < a.NsA ? 0 : 1;
     };
-    if (!mbar_wait(&s_bar, 0, a.spin_limit)) {
-        if (threadIdx.x == 0) atomicOr(a.error, 2);
+    if (!mbar_wait(&s_bar, 0, a.spin_limit)) s_fail = 1;
+    __syncthreads();
+    if (s_fail) {  // every thread leaves here: the factor tiles still land in this block's memory first
+        if (threadIdx.x == 0) {
+            atomicOr(a.error, 2);
+            mbar_wait(&s_bar, 0, kDrainSpins);
+        }
         return;
     }
 

@@ -422,6 +422,8 @@ struct scft_solver_s {
     int kind = 0;
     int precision = SCFT_FP64;
     int device = 0;
+    int users = 0;                 // iteration contexts (scft_diblock_t) built on this solver
+    bool destroy_pending = false;  // scft_solver_destroy was called while users > 0
     int sms = 0;                   // multiprocessors of `device` (queried on first use)
     size_t axis_dmma_smem_set = 0; // dynamic shared memory granted to the tensor-core axis passes
     size_t axis_tf32_smem_set = 0;
@@ -1105,6 +1107,10 @@ int scft_operator_terms(int kind, const size_t grid_size_log[3], const double tr
 
 int scft_solver_destroy(scft_solver_t s) {
     if (!s) return SCFT_OK;
+    if (s->users > 0) {  // iteration contexts still use it: freed with the last of them
+        s->destroy_pending = true;
+        return SCFT_OK;
+    }
     cudaSetDevice(s->device);
     cudaStreamSynchronize(s->stream);
     delete s;
@@ -1351,15 +1357,22 @@ int scft_diblock_create(scft_solver_t s, double fA, double ds, double xN, double
     CK(cudaMemset(d->phiA.p, 0, M * sizeof(double)));
     CK(cudaMemset(d->phiB.p, 0, M * sizeof(double)));
     CKR(diblock_buffers(d.get(), d->precision));
+    ++s->users;  // the solver outlives this context (scft_solver_destroy defers)
     *out = d.release();
     return SCFT_OK;
 }
 
 int scft_diblock_destroy(scft_diblock_t d) {
     if (!d) return SCFT_OK;
-    cudaSetDevice(d->solver->device);
-    cudaStreamSynchronize(d->solver->stream);
+    scft_solver_t s = d->solver;
+    cudaSetDevice(s->device);
+    cudaStreamSynchronize(s->stream);
     delete d;
+    --s->users;
+    if (s->destroy_pending && s->users == 0) {
+        s->destroy_pending = false;
+        return scft_solver_destroy(s);
+    }
     return SCFT_OK;
 }
 
@@ -1407,6 +1420,20 @@ int scft_diblock_set_mixing(scft_diblock_t d, int history, double beta) {
     }
     d->mix_history = history;
     d->mix_beta = history > 0 ? beta : 0.0;
+    return SCFT_OK;
+}
+
+int scft_diblock_set_wait_limit(scft_diblock_t d, long long spins) {
+    if (!d) return fail(SCFT_ERR_INVALID_ARG, "null handle");
+    if (spins < 1) return fail(SCFT_ERR_INVALID_ARG, "the wait limit must be >= 1");
+    CK(cudaSetDevice(d->solver->device));
+    CK(cudaStreamSynchronize(d->solver->stream));
+    if (spins != d->spin_limit) {
+        // the limit is a kernel argument of the captured iteration graphs (both precisions)
+        d->captured_gen = ~0ULL;
+        d->saved_gen[0] = d->saved_gen[1] = ~0ULL;
+        d->spin_limit = spins;
+    }
     return SCFT_OK;
 }
 

@@ -61,6 +61,8 @@ class DiblockSCFT:
         check(_lib.load().scft_diblock_get_contour_counts(self._h, ctypes.byref(a), ctypes.byref(b)))
         self.NsA, self.NsB = a.value, b.value
         self.M = solver.get_space_size_phy()
+        self.iterations_done = 0       # iterations run through this object (checkpoints record it)
+        self.mixing = ["simple"]        # or ["anderson", history, beta]
 
     def close(self):
         if getattr(self, "_h", None):
@@ -95,6 +97,7 @@ class DiblockSCFT:
         parts = np.empty((n_iter, 4))
         check(_lib.load().scft_diblock_iterate(self._h, int(n_iter), _lib.dptr(F), _lib.dptr(parts),
                                                _lib.dptr(mi), _lib.dptr(Q)))
+        self.iterations_done += int(n_iter)
         return {"F": F, "parts": parts, "maxinc": mi, "Q": Q}
 
     def iterate_host(self, wA, wB, n_iter: int):
@@ -105,6 +108,7 @@ class DiblockSCFT:
         check(_lib.load().scft_diblock_iterate_host(self._h, _lib.dptr(wA), _lib.dptr(wB), int(n_iter),
                                                     _lib.dptr(phiA), _lib.dptr(phiB), _lib.dptr(F),
                                                     _lib.dptr(parts), _lib.dptr(mi), _lib.dptr(Q)))
+        self.iterations_done += int(n_iter)
         return {"F": F, "parts": parts, "maxinc": mi, "Q": Q, "phiA": phiA, "phiB": phiB}
 
     def device_fields(self):
@@ -143,10 +147,16 @@ class DiblockSCFT:
         starts empty)."""
         if kind == "simple":
             check(_lib.load().scft_diblock_set_mixing(self._h, 0, 0.0))
+            self.mixing = ["simple"]
         elif kind == "anderson":
             check(_lib.load().scft_diblock_set_mixing(self._h, int(history), float(beta)))
+            self.mixing = ["anderson", int(history), float(beta)]
         else:
             raise ValueError(f"unknown mixing {kind!r}")
+
+    def set_wait_limit(self, spins: int = 20_000_000):
+        """Poll limit of the contour kernels' bounded waits (see scft_diblock_set_wait_limit)."""
+        check(_lib.load().scft_diblock_set_wait_limit(self._h, int(spins)))
 
     def residuals(self) -> np.ndarray:
         """rms residual sqrt(<r, r> / 2M) of each iteration of the last iterate() call."""
@@ -155,6 +165,12 @@ class DiblockSCFT:
         out = np.empty(n.value)
         check(_lib.load().scft_diblock_get_residuals(self._h, _lib.dptr(out), n.value, ctypes.byref(n)))
         return out
+
+    def save_checkpoint(self, path):
+        """Binary checkpoint of this run (crysscft_sample_b200.checkpoint)."""
+        from . import checkpoint
+
+        checkpoint.save(self, path)
 
     def iterate_polished(self, n_iter: int, n_polish: int):
         """The precision form: n_iter - n_polish FP32 iterations, then n_polish FP64 ones."""

@@ -154,6 +154,7 @@ class CrysPSSolverPmmm(CrysPSSolverBase):
 
     def __init__(self, grid_size_log, precision: str = "fp64", device: int = -1, anisotropic: bool = False):
         super().__init__(grid_size_log, None, precision, device)
+        self.anisotropic = bool(anisotropic)
         if anisotropic:
             # orthorhombic cell (Lx, Ly, Lz); the reference's PMMM solver is cubic
             check(_lib.load().scft_solver_set_pmmm_anisotropic(self._h, 1))

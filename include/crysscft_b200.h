@@ -77,7 +77,9 @@ const char* scft_version(void);
  * device: CUDA ordinal (-1 = current device). */
 int scft_solver_create(int kind, const size_t grid_size_log[3], const double translational_part[9],
                        int precision, int device, scft_solver_t* out);
-/* Destructor (~CrysPSSolverP1 etc.).  NULL is accepted. */
+/* Destructor (~CrysPSSolverP1 etc.).  NULL is accepted.  While iteration contexts
+ * (scft_diblock_t) built on the solver exist, the solver stays alive and is freed with
+ * the last of them, so the two may be destroyed in either order. */
 int scft_solver_destroy(scft_solver_t solver);
 
 /* Host-only, no device work (callable on a machine without a GPU): the per-axis
@@ -198,6 +200,13 @@ int scft_diblock_get_precision(scft_diblock_t d, int* out);
  * + beta (r_0 + sum_j c_j (r_j - r_0)); a singular system restarts the history.
  * The history is cleared by this call and by scft_diblock_set_fields. */
 int scft_diblock_set_mixing(scft_diblock_t d, int history, double beta);
+
+/* Poll limit of every bounded wait inside the contour kernels (release flags, grid
+ * barriers, tile loads; default 20,000,000, about a second).  A wait that runs out makes
+ * the kernel record an error, let its own copies land and return, and the iteration call
+ * returns SCFT_ERR_TIMEOUT; the context stays usable.  No counterpart in the reference
+ * (it has no device code); a small limit is how the timeout path is tested. */
+int scft_diblock_set_wait_limit(scft_diblock_t d, long long spins);
 
 /* rms residual sqrt(<r, r> / 2M) of each iteration of the last scft_diblock_iterate
  * call (any mixing); *count = number of iterations, at most `capacity` copied. */
