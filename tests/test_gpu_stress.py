@@ -121,3 +121,36 @@ def test_cell_relaxation_reduces_stress(gpu):
                           4.0, n_outer=6, n_inner=10, step=2.0, tol=0.0)
     g = [abs(hh[2]) for hh in out["history"]]
     assert g[-1] < g[0]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_dlnQ_dL_at_128_bcc_matches_central_differences(gpu, precision):
+    # the bench system (128^3 BCC, PMMM on 64^3, ds = 0.005); "fp32": FP32 iterations, then
+    # the FP64 polish iteration whose stored contour the backward pass uses
+    N, L, ds = (128, 128, 128), 4.2, 0.005
+    wA, wB = fields.seed_fields(N, L, "BCC")
+    a, b = fields.to_physical("PMMM", wA), fields.to_physical("PMMM", wB)
+    G = solvers.make_solver("PMMM", N)
+    G.set_cell_para((L, L, L))
+    run = scft.DiblockSCFT(G, 0.25, ds, 20.0, 0.1)
+    run.set_fields(a, b)
+    if precision == "fp32":
+        run.set_precision("fp32")
+        run.iterate(5)
+        run.set_precision("fp64")
+    f = run.get_fields()
+    run.set_fields(f["wA"], f["wB"])
+    run.iterate(1)
+    g = run.stress()["dlnQ_dL"].sum()
+    run.close()
+    lnQ = []
+    hstep = 1e-5 * L
+    for sgn in (1, -1):
+        Lp = L + sgn * hstep
+        G.set_cell_para((Lp, Lp, Lp))
+        r = scft.DiblockSCFT(G, 0.25, ds, 20.0, 0.1)
+        r.set_fields(f["wA"], f["wB"])
+        lnQ.append(np.log(r.iterate(1)["Q"][0]))
+        r.close()
+    fd = (lnQ[0] - lnQ[1]) / (2 * hstep)
+    assert abs(fd - g) <= 1e-6 * abs(g) + 1e-10
