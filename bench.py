@@ -433,6 +433,7 @@ def run_batch(args):
     alg = replicas.sum_over_ranks(dist, sum(2 * (int(c["fA"] / ds) + int((1 - c["fA"]) / ds)) * 3 * np.prod(c["N"]) / 8 * 8
                                             for c in mine))
     value = n_inst * args.steps / dt
+    launches = int(replicas.sum_over_ranks(dist, B.launches_per_iteration() * args.steps))
     # end to end: fields of every instance copied in and phi copied out every step
     host = [B.get_fields(i) for i in range(len(mine))]
     t0 = time.perf_counter()
@@ -458,7 +459,7 @@ def run_batch(args):
                                    "chiN~U[14,30], fA~U[0.2,0.35], L~U[3.8,5.5], ds=0.01, BCC or FCC",
                        "autotuned": tuned, "parallelism": f"instances sharded over {world} GPU(s)",
                        "l2": "working set (all contour stores) larger than L2"},
-            "gpu_launches": None,
+            "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": None, "kernel": "one batch iteration (graph of all instances)"},
             "e2e": {"value": n_inst * k_e2e / e2e_dt, "unit": "instance-iterations/s",

@@ -90,6 +90,17 @@ class BatchSCFT:
         check(_lib.load().scft_batch_iterate(self._h, int(n_iter), _lib.dptr(F), _lib.dptr(mi)))
         return {"F": F, "maxinc": mi}
 
+    def launches_per_iteration(self) -> int:
+        """Kernel launches one batch iteration issues (summed over the instances' plans)."""
+        total = 0
+        for i in range(self.n):
+            d = ctypes.c_void_p()
+            check(_lib.load().scft_batch_instance(self._h, i, ctypes.byref(d)))
+            k = ctypes.c_size_t()
+            check(_lib.load().scft_diblock_launches_per_iteration(d, ctypes.byref(k)))
+            total += k.value
+        return total
+
     def configure(self, nstreams: int, form: int = 0):
         check(_lib.load().scft_batch_configure(self._h, int(nstreams), int(form)))
 
