@@ -117,7 +117,38 @@ q_reduce_kernel(const T* __restrict__ qc0, long long M, double* __restrict__ par
 }
 
 // phi_A = sum_{u=0}^{NsA} w_u fA/(NsA Q) q[u] q+[u];  phi_B over u = NsA..NsA+NsB.
-// q (forward chain) and qc (backward chain) hold U+1 = NsA+NsB+1 slices of M.
+// q (forward chain) and qc (backward chain) hold U+1 = NsA+NsB+1 slices of M.  Each thread
+// takes two neighbouring points (16-byte loads for FP64) and the slice loop is unrolled so
+// several slices' loads are in flight; the sum runs over the slices in order.  The stored
+// contour is read once, with streaming loads (it is larger than L2).
+template <typename T>
+struct Pair;
+template <>
+struct Pair<double> {
+    using type = double2;
+};
+template <>
+struct Pair<float> {
+    using type = float2;
+};
+
+template <typename T>
+__device__ __forceinline__ void phi_point_pair(const T* __restrict__ q, const T* __restrict__ qc, long long M,
+                                               long long i, long long s0, long long ns, double c, double& a0,
+                                               double& a1) {
+    using P = typename Pair<T>::type;
+#pragma unroll 4
+    for (long long s = 0; s <= ns; ++s) {
+        double factor = s == 0 ? 0.5 : (s == ns ? 0.5 : 1);
+        factor *= c;
+        const long long o = (s0 + s) * M + i;
+        const P x = __ldcs(reinterpret_cast<const P*>(q + o));
+        const P y = __ldcs(reinterpret_cast<const P*>(qc + o));
+        a0 += factor * (double)x.x * (double)y.x;
+        a1 += factor * (double)x.y * (double)y.y;
+    }
+}
+
 template <typename T>
 __global__ void phi_kernel(const T* __restrict__ q, const T* __restrict__ qc, double* __restrict__ phiA,
                            double* __restrict__ phiB, const IterState* st, double fA, long long NsA,
@@ -126,23 +157,35 @@ __global__ void phi_kernel(const T* __restrict__ q, const T* __restrict__ qc, do
     const double fB = 1 - fA;
     const double cA = fA / (NsA * Q);
     const double cB = fB / (NsB * Q);
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < M;
-         i += (long long)gridDim.x * blockDim.x) {
-        double a = 0.0;
-        for (long long s = 0; s <= NsA; ++s) {
-            double factor = s == 0 ? 0.5 : (s == NsA ? 0.5 : 1);
-            factor *= cA;
-            a += factor * (double)q[s * M + i] * (double)qc[s * M + i];
+    if (M & 1) {  // odd M: pairs would straddle slices unaligned; one point per thread
+        for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < M;
+             i += (long long)gridDim.x * blockDim.x) {
+            double a = 0.0, b = 0.0;
+            for (long long s = 0; s <= NsA; ++s) {
+                double factor = s == 0 ? 0.5 : (s == NsA ? 0.5 : 1);
+                factor *= cA;
+                a += factor * (double)q[s * M + i] * (double)qc[s * M + i];
+            }
+            for (long long s = 0; s <= NsB; ++s) {
+                double factor = s == 0 ? 0.5 : (s == NsB ? 0.5 : 1);
+                factor *= cB;
+                const long long u = NsA + s;
+                b += factor * (double)q[u * M + i] * (double)qc[u * M + i];
+            }
+            phiA[i] = a;
+            phiB[i] = b;
         }
-        double b = 0.0;
-        for (long long s = 0; s <= NsB; ++s) {
-            double factor = s == 0 ? 0.5 : (s == NsB ? 0.5 : 1);
-            factor *= cB;
-            const long long u = NsA + s;
-            b += factor * (double)q[u * M + i] * (double)qc[u * M + i];
-        }
-        phiA[i] = a;
-        phiB[i] = b;
+        return;
+    }
+    const long long pairs = M / 2;
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < pairs;
+         j += (long long)gridDim.x * blockDim.x) {
+        const long long i = 2 * j;
+        double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
+        phi_point_pair<T>(q, qc, M, i, 0, NsA, cA, a0, a1);
+        phi_point_pair<T>(q, qc, M, i, NsA, NsB, cB, b0, b1);
+        *reinterpret_cast<double2*>(phiA + i) = make_double2(a0, a1);
+        *reinterpret_cast<double2*>(phiB + i) = make_double2(b0, b1);
     }
 }
 

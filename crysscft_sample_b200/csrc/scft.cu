@@ -919,7 +919,7 @@ struct scft_diblock_s {
         const int rblocks = (int)std::min<long long>(kRedMaxBlocks, (MM + kRedThreads - 1) / kRedThreads);
         q_reduce_kernel<T><<<rblocks, kRedThreads, 0, st>>>(qc, MM, partials.p, state.p);
         CK(cudaGetLastError());
-        phi_kernel<T><<<blocks, 256, 0, st>>>(q, qc, phiA.p, phiB.p, state.p, fA, (long long)NsA,
+        phi_kernel<T><<<grid_blocks((MM + 1) / 2, 256), 256, 0, st>>>(q, qc, phiA.p, phiB.p, state.p, fA, (long long)NsA,
                                               (long long)NsB, MM);
         CK(cudaGetLastError());
         if (phase_events) CK(cudaEventRecord(phase_events[3], st));
