@@ -643,9 +643,10 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_kernel_ct(const Co
 //   plane phase (units (chain, x)):  [z y]  D  store q  D  [z y]  -> exchange buffer XP
 //   slab phase  (units (chain, y)):  [x]    D  store q  D  [x]    -> exchange buffer XS
 // Phase k (k = 0..U) finishes step k-1 (k >= 1) and starts step k (k < U); plane
-// phases have even k.  One grid barrier per step instead of two, and one exchange
-// round trip per step.  The Boltzmann-factor slices of the next phase are fetched
-// with cp.async before the barrier wait, so their latency hides behind it.
+// phases have even k.  One exchange per step and no grid barrier: a unit waits only for
+// the release flags of the units whose rows it reads.  The Boltzmann-factor tiles of the
+// next phase are loaded by TMA as soon as the current ones are consumed, and finished
+// q(s) tiles leave by TMA stores, so neither sits on the critical path.
 // ---------------------------------------------------------------------------
 namespace crysscft {
 

@@ -1,7 +1,7 @@
 // FP32 form of the alternating-layout contour kernel (precision form of the triplets).
 //
 // Same schedule as contour_alt_kernel (plane phases [A_z A_y], slab phases [A_x],
-// per-unit release flags, cp.async prefetch), with FP32 contour slices and
+// per-consumer release flags, TMA tiles), with FP32 contour slices and
 // Boltzmann factors.  The axis products run on the tensor cores as 3xTF32 split
 // products (mma.sync m16n8k8 .tf32, FP32 accumulate): every operand x is split
 // into hi = tf32(x) and lo = tf32(x - hi) and a*b ~ a_lo b_hi + a_hi b_lo + a_hi b_hi,
