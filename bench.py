@@ -330,16 +330,18 @@ def run_ours(args):
     # ---- end to end through the host-buffer ABI ---------------------------
     wA_h = torch.empty(M, dtype=torch.float64, pin_memory=True).numpy()
     wB_h = torch.empty(M, dtype=torch.float64, pin_memory=True).numpy()
+    phiA_h = torch.empty(M, dtype=torch.float64, pin_memory=True).numpy()
+    phiB_h = torch.empty(M, dtype=torch.float64, pin_memory=True).numpy()
     fA_, fB_ = run.get_fields()["wA"], run.get_fields()["wB"]
     wA_h[:] = fA_
     wB_h[:] = fB_
     k_e2e = max(10, args.steps // 5)
-    run.iterate_host(wA_h, wB_h, 1)
+    run.iterate_host(wA_h, wB_h, 1, phiA_h, phiB_h)
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(k_e2e):
-        run.iterate_host(wA_h, wB_h, 1)
+        run.iterate_host(wA_h, wB_h, 1, phiA_h, phiB_h)
     e1.record(stream)
     e1.synchronize()
     barrier()

@@ -100,9 +100,14 @@ class DiblockSCFT:
         self.iterations_done += int(n_iter)
         return {"F": F, "parts": parts, "maxinc": mi, "Q": Q}
 
-    def iterate_host(self, wA, wB, n_iter: int):
-        """End-to-end form: host fields in (updated in place), phi and history out."""
-        phiA, phiB = np.empty(self.M), np.empty(self.M)
+    def iterate_host(self, wA, wB, n_iter: int, phiA=None, phiB=None):
+        """End-to-end form: host fields in (updated in place), phi and history out.  phiA /
+        phiB may be given (e.g. page-locked arrays, for faster copies); else they are allocated."""
+        phiA = np.empty(self.M) if phiA is None else phiA
+        phiB = np.empty(self.M) if phiB is None else phiB
+        for a in (wA, wB, phiA, phiB):
+            if a.dtype != np.float64 or a.size != self.M or not a.flags.c_contiguous:
+                raise ValueError("host fields must be contiguous float64 arrays of the physical grid size")
         F, mi, Q = np.empty(n_iter), np.empty(n_iter), np.empty(n_iter)
         parts = np.empty((n_iter, 4))
         check(_lib.load().scft_diblock_iterate_host(self._h, _lib.dptr(wA), _lib.dptr(wB), int(n_iter),

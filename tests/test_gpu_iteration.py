@@ -82,3 +82,29 @@ def _compare(want, got):
     assert np.abs(got["phiA"] - want["phiA"]).max() < PHI_ATOL
     assert np.abs(got["phiB"] - want["phiB"]).max() < PHI_ATOL
     assert np.abs(got["wA"] - want["wA"]).max() < 1e-11
+
+
+def test_host_buffer_iteration_matches_device_iteration(gpu):
+    # the end-to-end form (fields in from host arrays, phi and fields back every call)
+    N, L = CFG0["N"], CFG0["L"]
+    wA, wB = fields.seed_fields(N, L, "BCC")
+    a, b = fields.to_physical("PMMM", wA).ravel(), fields.to_physical("PMMM", wB).ravel()
+
+    def ctx():
+        G = solvers.make_solver("PMMM", N)
+        G.set_cell_para((L, L, L))
+        return scft.DiblockSCFT(G, CFG0["fA"], CFG0["ds"], CFG0["xN"], CFG0["acc"])
+
+    dev = ctx()
+    dev.set_fields(a, b)
+    want = dev.iterate(3)
+    want.update(dev.get_fields())
+    host = ctx()
+    ha, hb = a.copy(), b.copy()
+    pa, pb = np.empty_like(ha), np.empty_like(hb)
+    F = []
+    for _ in range(3):
+        F.append(host.iterate_host(ha, hb, 1, pa, pb)["F"][0])
+    assert np.array_equal(np.array(F), want["F"])
+    assert np.array_equal(pa, want["phiA"]) and np.array_equal(pb, want["phiB"])
+    assert np.array_equal(ha, want["wA"]) and np.array_equal(hb, want["wB"])
