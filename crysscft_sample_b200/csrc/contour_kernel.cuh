@@ -538,6 +538,124 @@ __device__ __forceinline__ void col_op_ct(const double* __restrict__ F, double* 
     col_op_ct<R, C, LF, EO, kToSmem>(F, o, opE);
 }
 
+// ---- two even/odd levels (PMMM at n = 64) --------------------------------------------
+// For the PMMM operator the even half E = (A[i][j] + A[i][n-1-j]) / 2 is itself
+// centrosymmetric (it keeps only even frequencies: a DCT pair of half the size), so p = E u
+// splits again: ue = u_j + u_{h-1-j}, uo = u_j - u_{h-1-j} (j < h/2), pe = EE ue,
+// po = EO uo, p_i = pe_i + po_i, p_{h-1-i} = pe_i - po_i.  The odd half O stays dense.
+// Per warp: 16 rows (or columns) x 8 pair indices i and their three mirrors; 48 DMMA
+// instead of 64 per axis operation.  Operator block: [EE | EO] (h/2 x h/2, ld h/2 + 4),
+// then O (h x h, ld h + 4).
+template <int N>
+struct AxisShapeEO2 {
+    static constexpr int H = N / 2, H2 = N / 4;
+    static constexpr int LD2 = H2 + 4, LD = H + 4;
+    static constexpr int OFF_EO = H2 * LD2, OFF_O = 2 * H2 * LD2;
+    static constexpr int SIZE = OFF_O + H * LD;
+};
+
+// G[r][i] = sum_j F[r][j] A[i][j] on a 64 x 64 slab (two even/odd levels)
+template <int LF>
+__device__ __forceinline__ void row_op_eo2(const double* __restrict__ F, double* __restrict__ G,
+                                           const double* __restrict__ op) {
+    constexpr int C = 64;
+    using S = AxisShapeEO2<C>;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int rb = warp >> 1, hh = warp & 1;
+    const double* EEp = op + (8 * hh + g) * S::LD2 + t;
+    const double* EOp = EEp + S::OFF_EO;
+    const double* OA = op + S::OFF_O + (8 * hh + g) * S::LD + t;
+    const double* OB = op + S::OFF_O + (S::H - 1 - 8 * hh - g) * S::LD + t;
+    const double* Fr0 = F + (rb * 16 + g) * LF;
+    const double* Fr1 = Fr0 + 8 * LF;
+    double pe[2][2] = {}, po[2][2] = {}, rA[2][2] = {}, rB[2][2] = {};
+#pragma unroll
+    for (int k0 = 0; k0 < S::H2; k0 += 4) {
+        const int j = k0 + t;
+        const double s0 = Fr0[j] + Fr0[C - 1 - j], d0 = Fr0[S::H - 1 - j] + Fr0[S::H + j];
+        const double s1 = Fr1[j] + Fr1[C - 1 - j], d1 = Fr1[S::H - 1 - j] + Fr1[S::H + j];
+        const double bE = EEp[k0], bO = EOp[k0];
+        dmma884(pe[0], s0 + d0, bE);
+        dmma884(pe[1], s1 + d1, bE);
+        dmma884(po[0], s0 - d0, bO);
+        dmma884(po[1], s1 - d1, bO);
+    }
+#pragma unroll
+    for (int k0 = 0; k0 < S::H; k0 += 4) {
+        const int j = k0 + t;
+        const double v0 = Fr0[j] - Fr0[C - 1 - j], v1 = Fr1[j] - Fr1[C - 1 - j];
+        const double bA = OA[k0], bB = OB[k0];
+        dmma884(rA[0], v0, bA);
+        dmma884(rA[1], v1, bA);
+        dmma884(rB[0], v0, bB);
+        dmma884(rB[1], v1, bB);
+    }
+    const int ip = 8 * hh + 2 * t;
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+        double* Gr = G + (rb * 16 + a * 8 + g) * LF;
+        const double p10 = pe[a][0] + po[a][0], p11 = pe[a][1] + po[a][1];
+        const double p20 = pe[a][0] - po[a][0], p21 = pe[a][1] - po[a][1];
+        *reinterpret_cast<double2*>(Gr + ip) = make_double2(p10 + rA[a][0], p11 + rA[a][1]);
+        *reinterpret_cast<double2*>(Gr + C - 2 - ip) = make_double2(p11 - rA[a][1], p10 - rA[a][0]);
+        *reinterpret_cast<double2*>(Gr + S::H - 2 - ip) = make_double2(p21 + rB[a][1], p20 + rB[a][0]);
+        *reinterpret_cast<double2*>(Gr + S::H + ip) = make_double2(p20 - rB[a][0], p21 - rB[a][1]);
+    }
+}
+
+// G[i][c] = sum_j A[i][j] F[j][c] on a 64 x 64 slab (two even/odd levels); EPI as col_op_ct
+template <int LF, int EPI>
+__device__ __forceinline__ void col_op_eo2(const double* __restrict__ F, const ColOut& out,
+                                           const double* __restrict__ op) {
+    constexpr int R = 64;
+    using S = AxisShapeEO2<R>;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int cb = warp >> 1, hh = warp & 1;
+    const double* EEp = op + (8 * hh + g) * S::LD2 + t;
+    const double* EOp = EEp + S::OFF_EO;
+    const double* OA = op + S::OFF_O + (8 * hh + g) * S::LD + t;
+    const double* OB = op + S::OFF_O + (S::H - 1 - 8 * hh - g) * S::LD + t;
+    const double* Fc = F + cb * 16 + g;  // column c = cb*16 + b*8 + g
+    double pe[2][2] = {}, po[2][2] = {}, rA[2][2] = {}, rB[2][2] = {};
+#pragma unroll
+    for (int k0 = 0; k0 < S::H2; k0 += 4) {
+        const int j = k0 + t;
+        const double aE = EEp[k0], aO = EOp[k0];
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            const double* f = Fc + b * 8;
+            const double s = f[j * LF] + f[(R - 1 - j) * LF], d = f[(S::H - 1 - j) * LF] + f[(S::H + j) * LF];
+            dmma884(pe[b], aE, s + d);
+            dmma884(po[b], aO, s - d);
+        }
+    }
+#pragma unroll
+    for (int k0 = 0; k0 < S::H; k0 += 4) {
+        const int j = k0 + t;
+        const double aA = OA[k0], aB = OB[k0];
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            const double* f = Fc + b * 8;
+            const double v = f[j * LF] - f[(R - 1 - j) * LF];
+            dmma884(rA[b], aA, v);
+            dmma884(rB[b], aB, v);
+        }
+    }
+    const int ip = 8 * hh + g;
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+        const int c = cb * 16 + b * 8 + 2 * t;
+        const double p10 = pe[b][0] + po[b][0], p11 = pe[b][1] + po[b][1];
+        const double p20 = pe[b][0] - po[b][0], p21 = pe[b][1] - po[b][1];
+        col_store<LF, EPI>(out, ip, c, p10 + rA[b][0], p11 + rA[b][1]);
+        col_store<LF, EPI>(out, R - 1 - ip, c, p10 - rA[b][0], p11 - rA[b][1]);
+        col_store<LF, EPI>(out, S::H - 1 - ip, c, p20 + rB[b][0], p21 + rB[b][1]);
+        col_store<LF, EPI>(out, S::H + ip, c, p20 - rB[b][0], p21 - rB[b][1]);
+    }
+}
+
 // R x C slab between global (row stride gs) and shared memory (row stride LF), optional factor w
 template <bool TO_SMEM, int R, int C, int LF>
 __device__ __forceinline__ void move_slab_ct(double* sm, double* gm, long long gs, const double* w) {
@@ -774,10 +892,11 @@ __device__ __forceinline__ void tile_finish(double* T, const double* W0, const d
 // Shared-memory carve-up of the alternating kernel: operators, two padded work tiles
 // (row stride LF, conflict-free MMA fragments), and three dense N x N tiles filled and
 // drained by the bulk-copy engine (Boltzmann factors W0/W1, q staging tile QS).
-template <int N, bool EO>
+template <int N, bool EO, bool EO2 = false>
 struct AltShape {
     static constexpr int LF = N + 4;
-    static constexpr int OPS = 3 * AxisShape<N, EO>::SIZE;
+    static constexpr int AX = EO2 ? AxisShapeEO2<N>::SIZE : AxisShape<N, EO>::SIZE;  // per-axis operator block
+    static constexpr int OPS = 3 * AX;
     static constexpr int OPS_PAD = (OPS + 15) & ~15;        // 128-byte aligned tiles after it
     static constexpr int TILE = (N * LF + 15) & ~15;
     static constexpr int WT = N * N;
@@ -825,12 +944,13 @@ __device__ __forceinline__ void bulk_tile_store(T* q, const T* QS, int p, long l
     bulk_commit();
 }
 
-template <int N, bool EO>
+template <int N, bool EO, bool EO2 = false>
 __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const __grid_constant__ ContourArgs a) {
-    using S = AltShape<N, EO>;
+    static_assert(!EO2 || (EO && N == 64), "two even/odd levels: n = 64");
+    using S = AltShape<N, EO, EO2>;
     constexpr int LF = S::LF;
-    constexpr int OFFY = AxisShape<N, EO>::SIZE;
-    constexpr int OFFZ = 2 * AxisShape<N, EO>::SIZE;
+    constexpr int OFFY = S::AX;
+    constexpr int OFFZ = 2 * S::AX;
     constexpr int TPR = kContourThreads / N;         // threads per tile row (rows * TPR <= block)
     constexpr int CPT = (N / 2 + TPR - 1) / TPR;     // 16-byte chunks per thread and row
     constexpr unsigned TILE_BYTES = N * N * sizeof(double);
@@ -908,6 +1028,20 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
         if (warp == 0) bulk_wait_all();
     };
 
+    // axis operations on shared-memory tiles (two even/odd levels when EO2)
+    auto row_z = [&](const double* F, double* G) {
+        if constexpr (EO2) row_op_eo2<LF>(F, G, sops + OFFZ);
+        else row_op_ct<N, N, LF, EO>(F, G, sops + OFFZ);
+    };
+    auto col_smem = [&](const double* F, double* G, int off) {
+        if constexpr (EO2) col_op_eo2<LF, kToSmem>(F, ColOut{G, 0}, sops + off);
+        else col_op_ct<N, N, LF, EO>(F, G, sops + off);
+    };
+    auto col_global = [&](const double* F, const ColOut& o, int off) {
+        if constexpr (EO2) col_op_eo2<LF, kToGlobal>(F, o, sops + off);
+        else col_op_ct<N, N, LF, EO, kToGlobal>(F, o, sops + off);
+    };
+
     if (warp == 0) issue_w(0);
     for (int k = 0; k <= U; ++k) {
         const bool plane = (k & 1) == 0;
@@ -950,11 +1084,11 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
         if (k >= 1) {
             // finish step k-1: the axis ops this layout owns, then D, q(s+1) to the staging tile
             if (plane) {
-                row_op_ct<N, N, LF, EO>(cur, oth, sops + OFFZ);
+                row_z(cur, oth);
                 __syncthreads();
-                col_op_ct<N, N, LF, EO>(oth, cur, sops + OFFY);
+                col_smem(oth, cur, OFFY);
             } else {
-                col_op_ct<N, N, LF, EO>(cur, oth, sops);
+                col_smem(cur, oth, 0);
                 double* tmp = cur;
                 cur = oth;
                 oth = tmp;
@@ -986,11 +1120,11 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
             // which the other layout finishes next phase
             const ColOut xo{(plane ? XP : XS) + off, gs};
             if (plane) {
-                row_op_ct<N, N, LF, EO>(cur, oth, sops + OFFZ);
+                row_z(cur, oth);
                 __syncthreads();
-                col_op_ct<N, N, LF, EO, kToGlobal>(oth, xo, sops + OFFY);
+                col_global(oth, xo, OFFY);
             } else {
-                col_op_ct<N, N, LF, EO, kToGlobal>(cur, xo, sops);
+                col_global(cur, xo, 0);
             }
             __syncthreads();
             if (threadIdx.x < N) {  // tell consumer threadIdx.x that tile p of phase k is out

@@ -119,6 +119,10 @@ struct OpsSet {
     // even/odd axis E then O (h x h, leading dimension h+4), else A (n x n, n+4)
     std::vector<double> h_packed;
     DevBuf<double> d_packed;
+    // two even/odd levels (PMMM, n = 64 on every axis): per axis [EE | EO | O] (AxisShapeEO2)
+    std::vector<double> h_packed2;
+    DevBuf<double> d_packed2;
+    bool eo2 = false;
     int eo[3] = {0, 0, 0}, off[3] = {0, 0, 0}, ld[3] = {0, 0, 0}, half[3] = {0, 0, 0};
     int total = 0;
     // FP32 precision form: per axis [hi][lo] TF32 split parts, each E,O (even/odd) or A
@@ -218,6 +222,41 @@ void pack_operator(const std::vector<long double>& A, int n, OpsSet& s, int axis
             for (int j = 0; j < n; ++j) D[(size_t)i * ld + j] = (double)A[(size_t)i * n + j];
     }
     s.total = (int)s.h_packed.size();
+}
+
+// Append one axis operator in the two-level even/odd form when its even half is itself
+// centrosymmetric (PMMM) and n == 64; returns false (and appends nothing) otherwise.
+bool pack_operator_eo2(const std::vector<long double>& A, int n, OpsSet& s) {
+    if (n != 64) return false;
+    const int h = n / 2, h2 = n / 4;
+    std::vector<long double> E((size_t)h * h), O((size_t)h * h);
+    for (int i = 0; i < h; ++i)
+        for (int j = 0; j < h; ++j) {
+            const long double a = A[(size_t)i * n + j], b = A[(size_t)i * n + (n - 1 - j)];
+            E[(size_t)i * h + j] = (a + b) / 2;
+            O[(size_t)i * h + j] = (a - b) / 2;
+            if (fabsl(a - A[(size_t)(n - 1 - i) * n + (n - 1 - j)]) > 1e-17L * (1.0L + fabsl(a))) return false;
+        }
+    for (int i = 0; i < h; ++i)
+        for (int j = 0; j < h; ++j) {
+            const long double a = E[(size_t)i * h + j], b = E[(size_t)(h - 1 - i) * h + (h - 1 - j)];
+            if (fabsl(a - b) > 1e-17L * (1.0L + fabsl(a))) return false;
+        }
+    const int ld2 = h2 + 4, ld = h + 4;
+    const size_t base = s.h_packed2.size();
+    s.h_packed2.resize(base + 2 * (size_t)h2 * ld2 + (size_t)h * ld, 0.0);
+    double* EE = s.h_packed2.data() + base;
+    double* EO = EE + (size_t)h2 * ld2;
+    double* OO = EO + (size_t)h2 * ld2;
+    for (int i = 0; i < h2; ++i)
+        for (int j = 0; j < h2; ++j) {
+            const long double a = E[(size_t)i * h + j], b = E[(size_t)i * h + (h - 1 - j)];
+            EE[(size_t)i * ld2 + j] = (double)((a + b) / 2);
+            EO[(size_t)i * ld2 + j] = (double)((a - b) / 2);
+        }
+    for (int i = 0; i < h; ++i)
+        for (int j = 0; j < h; ++j) OO[(size_t)i * ld + j] = (double)O[(size_t)i * h + j];
+    return true;
 }
 
 int upload_operator(const std::vector<long double>& A, int n, OpsSet& s, int axis) {
@@ -354,7 +393,11 @@ ContourFnF contour_alt_kernel_f32_for(int n, int eo, size_t* smem) {
     return nullptr;
 }
 
-ContourFn contour_alt_kernel_for(int n, int eo, size_t* smem) {
+ContourFn contour_alt_kernel_for(int n, int eo, size_t* smem, bool eo2 = false) {
+    if (eo2 && eo && n == 64) {
+        *smem = AltShape<64, true, true>::SMEM;
+        return contour_alt_kernel<64, true, true>;
+    }
 #define CRYSSCFT_ALT(N, E)                     \
     {                                          \
         *smem = AltShape<N, E>::SMEM;          \
@@ -460,6 +503,7 @@ struct scft_solver_s {
         const int nt = nterms();
         s->nterms = nt;
         for (int t = 1; t < nt; ++t) s->more.push_back(std::make_unique<OpsSet>());
+        int eo2_axes = 0;
         for (int ax = 0; ax < 3; ++ax) {
             std::vector<long double> A;
             const int N = (int)grid_log[ax];
@@ -477,6 +521,13 @@ struct scft_solver_s {
             CKR(upload_operator(A, (int)grid_phy[ax], *s, ax));
             pack_operator(A, (int)grid_phy[ax], *s, ax);
             pack_operator_f32(A, (int)grid_phy[ax], *s, ax);
+            eo2_axes += (kind == SCFT_SOLVER_PMMM && nt == 1 && pack_operator_eo2(A, (int)grid_phy[ax], *s)) ? 1 : 0;
+        }
+        s->eo2 = eo2_axes == 3;
+        if (s->eo2) {
+            CKR(s->d_packed2.alloc(s->h_packed2.size()));
+            CK(cudaMemcpy(s->d_packed2.p, s->h_packed2.data(), s->h_packed2.size() * sizeof(double),
+                          cudaMemcpyHostToDevice));
         }
         CKR(s->d_packed.alloc(s->h_packed.size()));
         CK(cudaMemcpy(s->d_packed.p, s->h_packed.data(), s->h_packed.size() * sizeof(double),
@@ -685,6 +736,7 @@ struct scft_diblock_s {
     size_t persistent_smem = 0;
     ContourFn contour_fn = nullptr;
     bool alternating = false;             // contour_fn is the alternating-layout kernel
+    bool alt_eo2 = false;                 // ... in its two-level even/odd form (operators d_packed2)
     int force_form = 0;                   // 0 auto, 1 alternating, 2 two-phase, 3 per-axis kernels
     int last_form = 0;                    // force_form the current launch plan was built with
     DevBuf<double> d_xch;                 // exchange buffers, 2 x space_size_phy per chain
@@ -788,6 +840,7 @@ struct scft_diblock_s {
     int setup_persistent() {
         persistent = false;
         alternating = false;
+        alt_eo2 = false;
         if (force_form == 3) return SCFT_OK;  // per-axis kernels only
         if (solver->ops && solver->ops->nterms > 1) return SCFT_OK;  // multi-term: per-axis kernels
         if (precision == SCFT_FP32) return setup_persistent_f32();
@@ -808,11 +861,14 @@ struct scft_diblock_s {
         alternating = false;
         if (nx == ny && ny == nz && o->eo[0] == o->eo[1] && o->eo[1] == o->eo[2] && force_form != 2) {
             size_t alt_smem = 0;
-            ContourFn f = contour_alt_kernel_for(nx, o->eo[0], &alt_smem);
+            ContourFn f = contour_alt_kernel_for(nx, o->eo[0], &alt_smem, o->eo2);
+            alt_eo2 = f && o->eo2 && nx == 64;
             if (f && alt_smem <= (size_t)dev_smem) {
                 contour_fn = f;
                 smem = alt_smem;
                 alternating = true;
+            } else {
+                alt_eo2 = false;
             }
         }
         if (!d_xch.p) CKR(d_xch.alloc(4 * M));
@@ -842,7 +898,7 @@ struct scft_diblock_s {
         a.wds[1] = wBds;
         a.xbuf[0] = d_xch.p;          // 2M per chain: plane- and slab-phase exchange buffers
         a.xbuf[1] = d_xch.p + 2 * M;
-        a.ops = o->d_packed.p;
+        a.ops = alt_eo2 ? o->d_packed2.p : o->d_packed.p;
         for (int ax = 0; ax < 3; ++ax) {
             a.n[ax] = (int)solver->grid_phy[ax];
             a.eo[ax] = o->eo[ax];
