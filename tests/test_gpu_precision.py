@@ -27,8 +27,9 @@ def _pair(kind, N, nstep, npolish, L=4.2, fA=0.25, xN=20.0, ds=0.01, acc=0.1):
 
 
 @pytest.mark.parametrize("kind,N", [("PMMM", (32, 32, 32)), ("3M", (32, 32, 32)), ("P1", (32, 32, 32)),
-                                    ("PMMM", (64, 64, 64))])
+                                    ("PMMM", (64, 64, 64)), ("PMMM", (128, 128, 128))])
 def test_fp32_triplets_track_fp64(gpu, kind, N):
+    # PMMM 128^3 (64^3 physical) is the FP32 contour kernel of the 128^3 BCC benchmark
     want, got = _pair(kind, N, 6, 1)
     rel = np.abs(got["F"] - want["F"]) / np.abs(want["F"])
     assert rel[:-1].max() < FP32_REL          # FP32 iterations
