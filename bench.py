@@ -301,9 +301,12 @@ def run_ours(args):
     # per triplet: read q(s), read exp(-w ds/2), write q(s+1); K generated on chip, not counted
     alg_bytes_launch = 2 * U * 3 * M * b
     achieved = alg_bytes_launch / chain_s / 1e9
-    # FP64 multiply-adds of the triplets: per point and axis n/2 (even/odd operators) or n
+    # FP64 multiply-adds the contour kernel executes per point and axis: n/2 with the
+    # even/odd operators, 3n/8 with two even/odd levels (PMMM, 64 points on every axis), else n
     n_phy = solver.get_grid_size_phy()
-    per_point = sum((v // 2) if (args.solver != "3M" and v % 16 == 0) else v for v in n_phy)
+    two_level = args.solver == "PMMM" and all(v == 64 for v in n_phy)
+    per_point = sum((3 * v // 8) if two_level else (v // 2) if (args.solver != "3M" and v % 16 == 0) else v
+                    for v in n_phy)
     flops_launch = 2.0 * 2 * U * M * per_point
     import ctypes as _ct
 
@@ -370,7 +373,9 @@ def run_ours(args):
                          "fp64": {"achieved_tflops": flops_launch / chain_s / 1e12,
                                   "peak_tflops": tens.value, "peak_simt_tflops": simt.value,
                                   "frac": flops_launch / chain_s / 1e12 / tens.value,
-                                  "peak_source": "measured live (scft_measure_fp64_peak, FP64 m8n8k4 MMA)"}},
+                                  "flops_per_launch": flops_launch,
+                                  "peak_source": "measured live (scft_measure_fp64_peak, FP64 m8n8k4 MMA)"}
+                         if args.precision == "fp64" else None},
             "e2e": {"value": e2e_value, "unit": "iterations/s", "h2d_bytes_per_step": 2 * M * 8,
                     "d2h_bytes_per_step": 4 * M * 8 + 8 * 8},
             "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"],
