@@ -23,6 +23,21 @@ namespace crysscft {
 constexpr int kRowsZ = 32;
 constexpr int kColsYX = 32;
 
+// Copy an axis operator block (count values) into shared memory as 16-byte cp.async
+// chunks, all in flight at once (a plain load/store loop serialises ~35 global round trips
+// per thread at every launch); the caller waits with cp_async_wait_all + a barrier.
+template <typename T>
+__device__ __forceinline__ void op_copy_async(T* sop, const T* op, int count) {
+    const int bytes = count * (int)sizeof(T);
+    if ((reinterpret_cast<unsigned long long>(op) & 15) == 0 && (smem_u32(sop) & 15) == 0 && (bytes & 15) == 0) {
+        for (int i = threadIdx.x; i < bytes / 16; i += kContourThreads)
+            cp_async16(reinterpret_cast<char*>(sop) + 16 * i, reinterpret_cast<const char*>(op) + 16 * i);
+        cp_async_commit();
+    } else {
+        for (int i = threadIdx.x; i < count; i += kContourThreads) sop[i] = op[i];
+    }
+}
+
 struct AxisPassD {
     const double* in[2];
     double* out[2];
@@ -71,7 +86,7 @@ __global__ void __launch_bounds__(kContourThreads, 1) axis_dmma_kernel(const Axi
     double* sop = axs;
     double* F = axs + S::OPS;
     double* G = F + S::TILE_PAD;
-    for (int i = threadIdx.x; i < AxisShape<N, EO>::SIZE; i += kContourThreads) sop[i] = p.op[i];
+    op_copy_async(sop, p.op, AxisShape<N, EO>::SIZE);
 
     const int tiles = p.nchain * TL::TILES_PER_CHAIN;
     double2 v[PT], w[PT];
@@ -91,7 +106,8 @@ __global__ void __launch_bounds__(kContourThreads, 1) axis_dmma_kernel(const Axi
         }
     };
     int t = blockIdx.x;
-    if (t < tiles) fetch(t);
+    if (t < tiles) fetch(t);  // in flight with the operator copies
+    cp_async_wait_all();      // the operator; the loop's first barrier publishes it
     for (; t < tiles; t += gridDim.x) {
         const int c = t / TL::TILES_PER_CHAIN;
         const long long o = TL::origin(t - c * TL::TILES_PER_CHAIN);
@@ -167,7 +183,7 @@ __global__ void __launch_bounds__(kContourThreads) axis_tf32_kernel(const AxisPa
     float* sop = axf;
     float* F = axf + S::OPS;
     float* G = F + S::TILE_PAD;
-    for (int i = threadIdx.x; i < AxisShapeF<N, EO>::SIZE; i += kContourThreads) sop[i] = p.op[i];
+    op_copy_async(sop, p.op, AxisShapeF<N, EO>::SIZE);
 
     const int tiles = p.nchain * TL::TILES_PER_CHAIN;
     float4 v[PT], w[PT];
@@ -186,7 +202,8 @@ __global__ void __launch_bounds__(kContourThreads) axis_tf32_kernel(const AxisPa
         }
     };
     int t = blockIdx.x;
-    if (t < tiles) fetch(t);
+    if (t < tiles) fetch(t);  // in flight with the operator copies
+    cp_async_wait_all();      // the operator; the loop's first barrier publishes it
     for (; t < tiles; t += gridDim.x) {
         const int c = t / TL::TILES_PER_CHAIN;
         const long long o = TL::origin(t - c * TL::TILES_PER_CHAIN);
