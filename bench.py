@@ -301,10 +301,11 @@ def run_ours(args):
     # per triplet: read q(s), read exp(-w ds/2), write q(s+1); K generated on chip, not counted
     alg_bytes_launch = 2 * U * 3 * M * b
     achieved = alg_bytes_launch / chain_s / 1e9
-    # FP64 multiply-adds the contour kernel executes per point and axis: n/2 with the
-    # even/odd operators, 3n/8 with two even/odd levels (PMMM, 64 points on every axis), else n
+    # FP64 multiply-adds the triplet kernels execute per point and axis: n/2 with the
+    # even/odd operators, 3n/8 with two even/odd levels (PMMM, 64 or 128 points on every
+    # axis), else n
     n_phy = solver.get_grid_size_phy()
-    two_level = args.solver == "PMMM" and all(v == 64 for v in n_phy)
+    two_level = args.solver == "PMMM" and n_phy[0] in (64, 128) and all(v == n_phy[0] for v in n_phy)
     per_point = sum((3 * v // 8) if two_level else (v // 2) if (args.solver != "3M" and v % 16 == 0) else v
                     for v in n_phy)
     flops_launch = 2.0 * 2 * U * M * per_point

@@ -2,8 +2,9 @@
 // whole-contour kernels do not fit in shared memory: one persistent launch per pass
 // (z, y or x) over both contour chains, the axis operator resident in shared memory
 // (even/odd form when centrosymmetric), DMMA tiles from the contour kernel
-// (row_op_ct / col_op_ct), and the next tile prefetched into registers while the
-// current one is on the tensor cores.  The Boltzmann factor exp(-w ds/2) of the
+// (row_op_ct / col_op_ct; two even/odd levels, row_op_eo2 / col_op_eo2, for 128-point
+// PMMM axes), and the next tile prefetched into registers while the current one is on
+// the tensor cores.  The Boltzmann factor exp(-w ds/2) of the
 // contour step is applied on the z-pass input (pre) and the x-pass output (post),
 // as in the per-axis SIMT kernels (axis_kernels.cuh) these replace for such grids.
 //
@@ -23,33 +24,20 @@ namespace crysscft {
 constexpr int kRowsZ = 32;
 constexpr int kColsYX = 32;
 
-// Copy an axis operator block (count values) into shared memory as 16-byte cp.async
-// chunks, all in flight at once (a plain load/store loop serialises ~35 global round trips
-// per thread at every launch); the caller waits with cp_async_wait_all + a barrier.
-template <typename T>
-__device__ __forceinline__ void op_copy_async(T* sop, const T* op, int count) {
-    const int bytes = count * (int)sizeof(T);
-    if ((reinterpret_cast<unsigned long long>(op) & 15) == 0 && (smem_u32(sop) & 15) == 0 && (bytes & 15) == 0) {
-        for (int i = threadIdx.x; i < bytes / 16; i += kContourThreads)
-            cp_async16(reinterpret_cast<char*>(sop) + 16 * i, reinterpret_cast<const char*>(op) + 16 * i);
-        cp_async_commit();
-    } else {
-        for (int i = threadIdx.x; i < count; i += kContourThreads) sop[i] = op[i];
-    }
-}
-
 struct AxisPassD {
     const double* in[2];
     double* out[2];
     const double* pre[2];   // z pass: input *= pre (nullptr: none)
     const double* post[2];  // x pass: output *= post (nullptr: none)
-    const double* op;       // this axis' packed operator (AxisShape<N, EO> layout)
+    const double* op;       // this axis' packed operator (AxisShape<N, EO> or AxisShapeEO2<N> layout)
     int nchain;
 };
 
-template <int N, bool EO>
+template <int N, bool EO, bool EO2 = false>
 struct AxisDmmaShape {
-    static constexpr int OPS = (AxisShape<N, EO>::SIZE + 15) & ~15;
+    static_assert(!EO2 || (EO && N == 128), "two even/odd levels: 128-point even/odd axes");
+    static constexpr int OP_VALUES = EO2 ? AxisShapeEO2<N>::SIZE : AxisShape<N, EO>::SIZE;
+    static constexpr int OPS = (OP_VALUES + 15) & ~15;
     static constexpr int LFZ = N + 4;       // z tile: kRowsZ x N
     static constexpr int LFC = kColsYX + 4;  // y/x tile: N x kColsYX
     static constexpr int TILE = (N * LFC > kRowsZ * LFZ ? N * LFC : kRowsZ * LFZ);
@@ -75,9 +63,9 @@ struct AxisTiling {
     static constexpr int ROW_LEN = AX == 2 ? N : kColsYX;  // values per tile row
 };
 
-template <int N, bool EO, int AX>
+template <int N, bool EO, int AX, bool EO2 = false>
 __global__ void __launch_bounds__(kContourThreads, 1) axis_dmma_kernel(const AxisPassD p) {
-    using S = AxisDmmaShape<N, EO>;
+    using S = AxisDmmaShape<N, EO, EO2>;
     using TL = AxisTiling<N, AX>;
     constexpr int LF = AX == 2 ? S::LFZ : S::LFC;
     constexpr int RL = TL::ROW_LEN;
@@ -86,7 +74,7 @@ __global__ void __launch_bounds__(kContourThreads, 1) axis_dmma_kernel(const Axi
     double* sop = axs;
     double* F = axs + S::OPS;
     double* G = F + S::TILE_PAD;
-    op_copy_async(sop, p.op, AxisShape<N, EO>::SIZE);
+    op_copy_async(sop, p.op, S::OP_VALUES);
 
     const int tiles = p.nchain * TL::TILES_PER_CHAIN;
     double2 v[PT], w[PT];
@@ -132,8 +120,13 @@ __global__ void __launch_bounds__(kContourThreads, 1) axis_dmma_kernel(const Axi
         }
         __syncthreads();
         if (t + (int)gridDim.x < tiles) fetch(t + gridDim.x);  // in flight during the MMAs
-        if constexpr (AX == 2) row_op_ct<kRowsZ, N, LF, EO>(F, G, sop);
-        else col_op_ct<N, kColsYX, LF, EO>(F, G, sop);
+        if constexpr (AX == 2) {
+            if constexpr (EO2) row_op_eo2<kRowsZ, N, LF>(F, G, sop);
+            else row_op_ct<kRowsZ, N, LF, EO>(F, G, sop);
+        } else {
+            if constexpr (EO2) col_op_eo2<N, kColsYX, LF, kToSmem>(F, ColOut{G, 0}, sop);
+            else col_op_ct<N, kColsYX, LF, EO>(F, G, sop);
+        }
         __syncthreads();
         double* out = p.out[c] + o;
 #pragma unroll

@@ -25,6 +25,28 @@ namespace crysscft {
 constexpr int kContourThreads = 256;
 constexpr int kContourMaxN = 64;
 
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem_dst)), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Copy an operator block (count values) into shared memory as 16-byte cp.async chunks,
+// all in flight at once (a plain load/store loop serialises tens of global round trips
+// per thread at every launch); the caller waits with cp_async_wait_all + a barrier.
+template <typename T>
+__device__ __forceinline__ void op_copy_async(T* sop, const T* op, int count) {
+    const int bytes = count * (int)sizeof(T);
+    if ((reinterpret_cast<unsigned long long>(op) & 15) == 0 && (smem_u32(sop) & 15) == 0 && (bytes & 15) == 0) {
+        for (int i = threadIdx.x; i < bytes / 16; i += kContourThreads)
+            cp_async16(reinterpret_cast<char*>(sop) + 16 * i, reinterpret_cast<const char*>(op) + 16 * i);
+        cp_async_commit();
+    } else {
+        for (int i = threadIdx.x; i < count; i += kContourThreads) sop[i] = op[i];
+    }
+}
+
 struct ContourArgs {
     double* q[2];           // contour storage of each chain
     const double* wds[2];   // Boltzmann factors of block A (segments < NsA) and block B
@@ -302,7 +324,8 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_kernel_f64(const C
     double* sops = smem;
     double* F = smem + ops_pad;
     double* G = F + rows * lf;
-    for (int i = threadIdx.x; i < a.ops_total; i += kContourThreads) sops[i] = a.ops[i];
+    op_copy_async(sops, a.ops, a.ops_total);
+    cp_async_wait_all();
     __syncthreads();
 
     const long long M = (long long)nx * ny * nz;
@@ -538,31 +561,34 @@ __device__ __forceinline__ void col_op_ct(const double* __restrict__ F, double* 
     col_op_ct<R, C, LF, EO, kToSmem>(F, o, opE);
 }
 
-// ---- two even/odd levels (PMMM at n = 64) --------------------------------------------
+// ---- two even/odd levels (PMMM operators, n = 64 and 128) -----------------------------
 // For the PMMM operator the even half E = (A[i][j] + A[i][n-1-j]) / 2 is itself
 // centrosymmetric (it keeps only even frequencies: a DCT pair of half the size), so p = E u
 // splits again: ue = u_j + u_{h-1-j}, uo = u_j - u_{h-1-j} (j < h/2), pe = EE ue,
 // po = EO uo, p_i = pe_i + po_i, p_{h-1-i} = pe_i - po_i.  The odd half O stays dense.
-// Per warp: 16 rows (or columns) x 8 pair indices i and their three mirrors; 48 DMMA
-// instead of 64 per axis operation.  Operator block: [EE | EO] (h/2 x h/2, ld h/2 + 4),
-// then O (h x h, ld h + 4).
+// Per warp: 16 rows (or columns) x 8 pair indices i and their three mirrors; 3/4 of the
+// DMMA of one level.  Operator block: [EE | EO] (h/2 x h/2, ld h/2 + 4), then O (h x h,
+// ld h + 4).
 template <int N>
 struct AxisShapeEO2 {
     static constexpr int H = N / 2, H2 = N / 4;
     static constexpr int LD2 = H2 + 4, LD = H + 4;
     static constexpr int OFF_EO = H2 * LD2, OFF_O = 2 * H2 * LD2;
     static constexpr int SIZE = OFF_O + H * LD;
+    static constexpr int GROUPS = H2 / 8;  // groups of 8 pair indices
 };
 
-// G[r][i] = sum_j F[r][j] A[i][j] on a 64 x 64 slab (two even/odd levels)
-template <int LF>
+// G[r][i] = sum_j F[r][j] A[i][j] on an R x C slab (two even/odd levels); warp =
+// (16-row block, group of 8 pair indices), (R / 16) x (C / 32) warps
+template <int R, int C, int LF>
 __device__ __forceinline__ void row_op_eo2(const double* __restrict__ F, double* __restrict__ G,
                                            const double* __restrict__ op) {
-    constexpr int C = 64;
     using S = AxisShapeEO2<C>;
+    static_assert((R / 16) * S::GROUPS == kContourThreads / 32 && R % 16 == 0 && S::H2 % 8 == 0,
+                  "one warp per 16 rows x 8 pair indices");
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int g = lane >> 2, t = lane & 3;
-    const int rb = warp >> 1, hh = warp & 1;
+    const int rb = warp / S::GROUPS, hh = warp % S::GROUPS;
     const double* EEp = op + (8 * hh + g) * S::LD2 + t;
     const double* EOp = EEp + S::OFF_EO;
     const double* OA = op + S::OFF_O + (8 * hh + g) * S::LD + t;
@@ -604,15 +630,17 @@ __device__ __forceinline__ void row_op_eo2(const double* __restrict__ F, double*
     }
 }
 
-// G[i][c] = sum_j A[i][j] F[j][c] on a 64 x 64 slab (two even/odd levels); EPI as col_op_ct
-template <int LF, int EPI>
+// G[i][c] = sum_j A[i][j] F[j][c] on an R x C slab (two even/odd levels); EPI as col_op_ct;
+// warp = (16-column block, group of 8 pair indices), (C / 16) x (R / 32) warps
+template <int R, int C, int LF, int EPI>
 __device__ __forceinline__ void col_op_eo2(const double* __restrict__ F, const ColOut& out,
                                            const double* __restrict__ op) {
-    constexpr int R = 64;
     using S = AxisShapeEO2<R>;
+    static_assert((C / 16) * S::GROUPS == kContourThreads / 32 && C % 16 == 0 && S::H2 % 8 == 0,
+                  "one warp per 16 columns x 8 pair indices");
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int g = lane >> 2, t = lane & 3;
-    const int cb = warp >> 1, hh = warp & 1;
+    const int cb = warp / S::GROUPS, hh = warp % S::GROUPS;
     const double* EEp = op + (8 * hh + g) * S::LD2 + t;
     const double* EOp = EEp + S::OFF_EO;
     const double* OA = op + S::OFF_O + (8 * hh + g) * S::LD + t;
@@ -702,7 +730,8 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_kernel_ct(const Co
     double* sops = smem;
     double* F = smem + OPS_PAD;
     double* G = F + ROWS * LF;
-    for (int i = threadIdx.x; i < OPS; i += kContourThreads) sops[i] = a.ops[i];
+    op_copy_async(sops, a.ops, OPS);
+    cp_async_wait_all();
     __syncthreads();
 
     constexpr long long M = (long long)NX * NY * NZ;
@@ -768,15 +797,7 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_kernel_ct(const Co
 // ---------------------------------------------------------------------------
 namespace crysscft {
 
-__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem_src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-
 // ---- bulk-copy engine (cp.async.bulk, no tensor map) and mbarriers ----------------
-__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
@@ -985,7 +1006,8 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
             return;
         }
     }
-    for (int i = threadIdx.x; i < S::OPS; i += kContourThreads) sops[i] = a.ops[i];
+    op_copy_async(sops, a.ops, S::OPS);
+    cp_async_wait_all();
     if (threadIdx.x == 0) {
         s_fail = 0;
         mbar_init(&s_bar, 1);
@@ -1030,15 +1052,15 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
 
     // axis operations on shared-memory tiles (two even/odd levels when EO2)
     auto row_z = [&](const double* F, double* G) {
-        if constexpr (EO2) row_op_eo2<LF>(F, G, sops + OFFZ);
+        if constexpr (EO2) row_op_eo2<N, N, LF>(F, G, sops + OFFZ);
         else row_op_ct<N, N, LF, EO>(F, G, sops + OFFZ);
     };
     auto col_smem = [&](const double* F, double* G, int off) {
-        if constexpr (EO2) col_op_eo2<LF, kToSmem>(F, ColOut{G, 0}, sops + off);
+        if constexpr (EO2) col_op_eo2<N, N, LF, kToSmem>(F, ColOut{G, 0}, sops + off);
         else col_op_ct<N, N, LF, EO>(F, G, sops + off);
     };
     auto col_global = [&](const double* F, const ColOut& o, int off) {
-        if constexpr (EO2) col_op_eo2<LF, kToGlobal>(F, o, sops + off);
+        if constexpr (EO2) col_op_eo2<N, N, LF, kToGlobal>(F, o, sops + off);
         else col_op_ct<N, N, LF, EO, kToGlobal>(F, o, sops + off);
     };
 

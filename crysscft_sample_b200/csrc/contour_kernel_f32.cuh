@@ -416,7 +416,8 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel_f32(con
             bulk_tile_load<float, N>(WS + b * S::WT, a.wds[b], p, false, &a.tm_ws[b], &s_bar);
         }
     }
-    for (int i = threadIdx.x; i < S::OPS; i += kContourThreads) sops[i] = a.ops[i];
+    op_copy_async(sops, a.ops, S::OPS);
+    cp_async_wait_all();
     // block (0: A, 1: B) of the Boltzmann factor of step s
     auto blk_of = [&](int s) -> int {
         const long long in_slot = slot0 + (long long)dir * s;

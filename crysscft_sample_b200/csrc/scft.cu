@@ -119,7 +119,8 @@ struct OpsSet {
     // even/odd axis E then O (h x h, leading dimension h+4), else A (n x n, n+4)
     std::vector<double> h_packed;
     DevBuf<double> d_packed;
-    // two even/odd levels (PMMM, n = 64 on every axis): per axis [EE | EO | O] (AxisShapeEO2)
+    // two even/odd levels (PMMM, n = 64 or 128 on every axis): per axis [EE | EO | O]
+    // (AxisShapeEO2), x then y then z
     std::vector<double> h_packed2;
     DevBuf<double> d_packed2;
     bool eo2 = false;
@@ -225,9 +226,10 @@ void pack_operator(const std::vector<long double>& A, int n, OpsSet& s, int axis
 }
 
 // Append one axis operator in the two-level even/odd form when its even half is itself
-// centrosymmetric (PMMM) and n == 64; returns false (and appends nothing) otherwise.
+// centrosymmetric (PMMM) and n is 64 (whole-contour kernel) or 128 (axis passes); returns
+// false (and appends nothing) otherwise.
 bool pack_operator_eo2(const std::vector<long double>& A, int n, OpsSet& s) {
-    if (n != 64) return false;
+    if (n != 64 && n != 128) return false;
     const int h = n / 2, h2 = n / 4;
     std::vector<long double> E((size_t)h * h), O((size_t)h * h);
     for (int i = 0; i < h; ++i)
@@ -322,7 +324,13 @@ cudaError_t launch_axis(const AxisPass<T>& p, int nchain, bool contiguous, cudaS
 using AxisDmmaFn = void (*)(const AxisPassD);
 
 // The FP64 tensor-core axis pass for a cubic grid of side n (96 or 128); nullptr if none.
-AxisDmmaFn axis_dmma_kernel_for(int n, int eo, int ax, size_t* smem) {
+// eo2: the operators are in the two-level even/odd form (AxisShapeEO2, n = 128).
+AxisDmmaFn axis_dmma_kernel_for(int n, int eo, int ax, size_t* smem, bool eo2 = false) {
+    if (eo2 && eo && n == 128) {
+        *smem = AxisDmmaShape<128, true, true>::SMEM;
+        return ax == 0 ? axis_dmma_kernel<128, true, 0, true>
+                       : (ax == 1 ? axis_dmma_kernel<128, true, 1, true> : axis_dmma_kernel<128, true, 2, true>);
+    }
 #define CRYSSCFT_AXD(N, E)                                            \
     {                                                                 \
         *smem = AxisDmmaShape<N, E>::SMEM;                            \
@@ -469,6 +477,7 @@ struct scft_solver_s {
     bool destroy_pending = false;  // scft_solver_destroy was called while users > 0
     int sms = 0;                   // multiprocessors of `device` (queried on first use)
     size_t axis_dmma_smem_set = 0; // dynamic shared memory granted to the tensor-core axis passes
+    const void* axis_dmma_fn_set = nullptr;  // ... and to which kernel family (z pass)
     size_t axis_tf32_smem_set = 0;
     bool force_simt_axes = false;  // tests: run the SIMT per-axis kernels even where DMMA passes exist
     size_t grid_log[3] = {0, 0, 0};
@@ -608,13 +617,15 @@ struct scft_solver_s {
                 !force_simt_axes) {
                 AxisDmmaFn f[3];
                 size_t smem = 0;
-                for (int ax = 0; ax < 3; ++ax) f[ax] = axis_dmma_kernel_for(nx, ops->eo[ax], ax, &smem);
+                const bool eo2 = ops->eo2 && nx == 128;
+                for (int ax = 0; ax < 3; ++ax) f[ax] = axis_dmma_kernel_for(nx, ops->eo[ax], ax, &smem, eo2);
                 if (f[0] && f[1] && f[2]) {
                     if (!sms) CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-                    if (axis_dmma_smem_set != smem) {
+                    if (axis_dmma_smem_set != smem || axis_dmma_fn_set != (const void*)f[2]) {
                         for (int ax = 0; ax < 3; ++ax)
                             CK(cudaFuncSetAttribute(f[ax], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
                         axis_dmma_smem_set = smem;
+                        axis_dmma_fn_set = (const void*)f[2];
                     }
                     AxisPassD pz{}, py{}, px{};
                     for (int c = 0; c < nchain; ++c) {
@@ -623,9 +634,16 @@ struct scft_solver_s {
                         px.in[c] = t2[c]; px.out[c] = io[c].out; px.post[c] = io[c].post;
                     }
                     pz.nchain = py.nchain = px.nchain = nchain;
-                    pz.op = ops->d_packed.p + ops->off[2];
-                    py.op = ops->d_packed.p + ops->off[1];
-                    px.op = ops->d_packed.p + ops->off[0];
+                    if (eo2) {
+                        const size_t per_axis = ops->h_packed2.size() / 3;  // AxisShapeEO2<n>::SIZE
+                        pz.op = ops->d_packed2.p + 2 * per_axis;
+                        py.op = ops->d_packed2.p + per_axis;
+                        px.op = ops->d_packed2.p;
+                    } else {
+                        pz.op = ops->d_packed.p + ops->off[2];
+                        py.op = ops->d_packed.p + ops->off[1];
+                        px.op = ops->d_packed.p + ops->off[0];
+                    }
                     f[2]<<<sms, kContourThreads, smem, st>>>(pz);
                     CK(cudaGetLastError());
                     f[1]<<<sms, kContourThreads, smem, st>>>(py);
