@@ -772,7 +772,11 @@ struct scft_diblock_s {
     unsigned long long saved_gen[2] = {~0ULL, ~0ULL};
     bool saved_use_graph[2] = {true, true};
 
+    // page-locked staging of the end-to-end form: hist_cap history rows, then the error word
+    double* pin_out = nullptr;
+
     ~scft_diblock_s() {
+        if (pin_out) cudaFreeHost(pin_out);
         if (gexec) cudaGraphExecDestroy(gexec);
         if (graph) cudaGraphDestroy(graph);
         for (int i = 0; i < 2; ++i) {
@@ -1657,12 +1661,8 @@ static int diblock_prepare(scft_diblock_t d, bool want_graph) {
     return SCFT_OK;
 }
 
-// Read and clear the device-side error bits of the persistent kernel.
-static int diblock_check_device_error(scft_diblock_t d, cudaStream_t st) {
-    if (!d->ctrl.p) return SCFT_OK;
-    unsigned e = 0;
-    CK(cudaMemcpyAsync(&e, d->ctrl.p + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
+// Clear and report device-side error bits e of the persistent kernel (0: none).
+static int diblock_report_device_error(scft_diblock_t d, cudaStream_t st, unsigned e) {
     if (e) {
         CK(cudaMemsetAsync(d->ctrl.p + 1, 0, sizeof(unsigned), st));
         CK(cudaStreamSynchronize(st));
@@ -1672,6 +1672,37 @@ static int diblock_check_device_error(scft_diblock_t d, cudaStream_t st) {
                                           std::to_string(e) + ")");
     }
     return SCFT_OK;
+}
+
+// Read and clear the device-side error bits of the persistent kernel.
+static int diblock_check_device_error(scft_diblock_t d, cudaStream_t st) {
+    if (!d->ctrl.p) return SCFT_OK;
+    unsigned e = 0;
+    CK(cudaMemcpyAsync(&e, d->ctrl.p + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return diblock_report_device_error(d, st, e);
+}
+
+// Hand out `chunk` history rows h (iterations done .. done + chunk - 1) to the caller's
+// arrays; false if an iteration flagged Q <= 0 or a non-finite free energy.
+static bool diblock_take_history(scft_diblock_t d, const double* h, size_t chunk, size_t done, double* F,
+                                 double* parts, double* maxinc, double* Q) {
+    bool bad = false;
+    for (size_t i = 0; i < chunk; ++i) {
+        const double* r = &h[i * HIST_STRIDE];
+        if (F) F[done + i] = r[HIST_F];
+        if (parts) {
+            parts[4 * (done + i) + 0] = r[HIST_EH];
+            parts[4 * (done + i) + 1] = r[HIST_E0];
+            parts[4 * (done + i) + 2] = r[HIST_E1];
+            parts[4 * (done + i) + 3] = r[HIST_EK];
+        }
+        if (maxinc) maxinc[done + i] = r[HIST_MAXINC];
+        if (Q) Q[done + i] = r[HIST_Q];
+        d->last_residuals.push_back(r[HIST_RES]);
+        if (r[HIST_FLAGS] != 0.0) bad = true;
+    }
+    return !bad;
 }
 
 static int diblock_run(scft_diblock_t d, size_t n_iter, double* F, double* parts, double* maxinc,
@@ -1691,23 +1722,9 @@ static int diblock_run(scft_diblock_t d, size_t n_iter, double* F, double* parts
         CK(cudaStreamSynchronize(st));
         CKR(diblock_check_device_error(d, st));
         if (chunk) d->last_iter_precision = d->precision;
-        bool bad = false;
-        for (size_t i = 0; i < chunk; ++i) {
-            const double* r = &h[i * HIST_STRIDE];
-            if (F) F[done + i] = r[HIST_F];
-            if (parts) {
-                parts[4 * (done + i) + 0] = r[HIST_EH];
-                parts[4 * (done + i) + 1] = r[HIST_E0];
-                parts[4 * (done + i) + 2] = r[HIST_E1];
-                parts[4 * (done + i) + 3] = r[HIST_EK];
-            }
-            if (maxinc) maxinc[done + i] = r[HIST_MAXINC];
-            if (Q) Q[done + i] = r[HIST_Q];
-            d->last_residuals.push_back(r[HIST_RES]);
-            if (r[HIST_FLAGS] != 0.0) bad = true;
-        }
+        const bool ok = diblock_take_history(d, h.data(), chunk, done, F, parts, maxinc, Q);
         done += chunk;
-        if (bad) return fail(SCFT_ERR_NUMERIC, "Q <= 0 or a non-finite free energy in an iteration");
+        if (!ok) return fail(SCFT_ERR_NUMERIC, "Q <= 0 or a non-finite free energy in an iteration");
     }
     return SCFT_OK;
 }
@@ -1720,13 +1737,45 @@ int scft_diblock_iterate(scft_diblock_t d, size_t n_iter, double* F, double* par
     return diblock_run(d, n_iter, F, parts, maxinc, Q);
 }
 
+// Fields in, n_iter iterations, results out, all enqueued on the solver's stream with one
+// synchronisation at the end (history rows and the error word through page-locked
+// staging).  On an error the caller's phi/w arrays may already hold the failed
+// iteration's values; the return code says so.
 int scft_diblock_iterate_host(scft_diblock_t d, double* wA, double* wB, size_t n_iter, double* phiA,
                               double* phiB, double* F, double* parts, double* maxinc, double* Q) {
     if (!d || !wA || !wB) return fail(SCFT_ERR_INVALID_ARG, "null argument");
     CK(cudaSetDevice(d->solver->device));
-    CKR(scft_diblock_set_fields(d, wA, wB));
-    CKR(diblock_run(d, n_iter, F, parts, maxinc, Q));
-    return scft_diblock_get_fields(d, phiA, phiB, wA, wB);
+    if (n_iter > d->hist_cap) {  // more rows than one history buffer: the chunked path
+        CKR(scft_diblock_set_fields(d, wA, wB));
+        CKR(diblock_run(d, n_iter, F, parts, maxinc, Q));
+        return scft_diblock_get_fields(d, phiA, phiB, wA, wB);
+    }
+    if (!d->pin_out) CK(cudaMallocHost(&d->pin_out, ((size_t)d->hist_cap * HIST_STRIDE + 1) * sizeof(double)));
+    CKR(diblock_prepare(d, true));
+    cudaStream_t st = d->solver->stream;
+    const size_t b = d->M * sizeof(double);
+    CK(cudaMemcpyAsync(d->wA.p, wA, b, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d->wB.p, wB, b, cudaMemcpyHostToDevice, st));
+    if (d->and_state.p) CK(cudaMemsetAsync(d->and_state.p, 0, sizeof(AndersonState), st));  // new fields: no history
+    d->fields_set = true;
+    d->last_residuals.clear();
+    CK(cudaMemsetAsync(d->state.p, 0, sizeof(IterState), st));
+    for (size_t i = 0; i < n_iter; ++i) CKR(d->run_once(st));
+    double* h = d->pin_out;
+    unsigned* err = reinterpret_cast<unsigned*>(d->pin_out + (size_t)d->hist_cap * HIST_STRIDE);
+    *err = 0;
+    if (n_iter) CK(cudaMemcpyAsync(h, d->hist.p, n_iter * HIST_STRIDE * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (d->ctrl.p) CK(cudaMemcpyAsync(err, d->ctrl.p + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    if (phiA) CK(cudaMemcpyAsync(phiA, d->phiA.p, b, cudaMemcpyDeviceToHost, st));
+    if (phiB) CK(cudaMemcpyAsync(phiB, d->phiB.p, b, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(wA, d->wA.p, b, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(wB, d->wB.p, b, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    CKR(diblock_report_device_error(d, st, *err));
+    if (n_iter) d->last_iter_precision = d->precision;
+    if (!diblock_take_history(d, h, n_iter, 0, F, parts, maxinc, Q))
+        return fail(SCFT_ERR_NUMERIC, "Q <= 0 or a non-finite free energy in an iteration");
+    return SCFT_OK;
 }
 
 int scft_diblock_launches_per_iteration(scft_diblock_t d, size_t* out) {

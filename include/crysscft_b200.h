@@ -178,7 +178,10 @@ int scft_diblock_iterate(scft_diblock_t d, size_t n_iter, double* F, double* par
                          double* maxinc, double* Q);
 
 /* End-to-end form for callers that keep fields in host memory: copies wA/wB in, runs
- * n_iter iterations, copies phiA/phiB and the updated wA/wB (in place) back out. */
+ * n_iter iterations, copies phiA/phiB and the updated wA/wB (in place) back out, with one
+ * host synchronisation per call (page-locked wA/wB/phiA/phiB make the copies
+ * asynchronous).  F, parts, maxinc, Q as in scft_diblock_iterate.  If an error code is
+ * returned, phiA/phiB/wA/wB may already hold the values of the failed iteration. */
 int scft_diblock_iterate_host(scft_diblock_t d, double* wA, double* wB, size_t n_iter,
                               double* phiA, double* phiB, double* F, double* parts,
                               double* maxinc, double* Q);

@@ -108,3 +108,10 @@ def test_host_buffer_iteration_matches_device_iteration(gpu):
     assert np.array_equal(np.array(F), want["F"])
     assert np.array_equal(pa, want["phiA"]) and np.array_equal(pb, want["phiB"])
     assert np.array_equal(ha, want["wA"]) and np.array_equal(hb, want["wB"])
+    # several iterations in one call: every history row comes back
+    multi = ctx()
+    ma, mb = a.copy(), b.copy()
+    got = multi.iterate_host(ma, mb, 3)
+    for key in ("F", "Q", "maxinc", "parts"):
+        assert np.array_equal(got[key], want[key]), key
+    assert np.array_equal(got["phiA"], want["phiA"]) and np.array_equal(ma, want["wA"])
