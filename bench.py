@@ -145,6 +145,17 @@ def reference_iterations(args, n_iter: int, threads: int | None = None):
     return out["wall_seconds"] / n_iter, cores, out
 
 
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for row in f:
+                if row.startswith("model name"):
+                    return row.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -174,7 +185,8 @@ def run_reference_arm(args):
         "cpu_baseline": {"value": value, "unit": "iterations/s", "cores": cores, "kind": "reference",
                          "sample": (f"{k} full SCFT iteration(s) of the same workload ({2 * U} triplets each): "
                                     "the reference's C++ solvers and driver loop compiled with an FFTW-API "
-                                    f"shim (FFTW absent), OpenMP {cores} threads, wall {wall:.1f} s")},
+                                    f"shim (FFTW absent), OpenMP {cores} threads, wall {wall:.1f} s"),
+                         "cpu_model": cpu_model()},
         "e2e": {"value": value, "unit": "iterations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -398,7 +410,16 @@ def run_ours(args):
                 "value": 1.0 / per_it, "unit": "iterations/s", "cores": cores, "kind": "reference",
                 "sample": ("2 full SCFT iterations of the same workload: the reference's C++ solvers and "
                            "driver loop compiled with an FFTW-API shim (FFTW absent), OpenMP threads"),
+                "cpu_model": cpu_model(),
             }
+            # the reference's own setting (its driver calls omp_set_num_threads(1))
+            per_1, _, _ = reference_iterations(args, 1, threads=1)
+            from oracle import ref as _ref
+
+            _ref.set_num_threads(cores)
+            line["cpu_baseline"]["single_thread"] = {
+                "value": 1.0 / per_1, "unit": "iterations/s", "cores": 1,
+                "sample": "1 full SCFT iteration of the same workload, 1 OpenMP thread"}
         except Exception as e:  # the CPU baseline is reported, never required
             line["cpu_baseline"] = {"value": None, "unit": "iterations/s", "cores": 0, "kind": "reference",
                                     "sample": f"unavailable: {e}"}

@@ -479,7 +479,6 @@ struct scft_solver_s {
     size_t axis_dmma_smem_set = 0; // dynamic shared memory granted to the tensor-core axis passes
     const void* axis_dmma_fn_set = nullptr;  // ... and to which kernel family (z pass)
     size_t axis_tf32_smem_set = 0;
-    bool force_simt_axes = false;  // tests: run the SIMT per-axis kernels even where DMMA passes exist
     size_t grid_log[3] = {0, 0, 0};
     size_t grid_phy[3] = {0, 0, 0};
     size_t M = 0;
@@ -613,8 +612,7 @@ struct scft_solver_s {
                 return fail(SCFT_ERR_INVALID_ARG, "multi-term triplet: input and output alias");
         if constexpr (sizeof(T) == 8) {
             // large cubic grids: the three passes on the FP64 tensor cores (axis_dmma.cuh)
-            if (nt == 1 && nx == ny && ny == nz && ops->eo[0] == ops->eo[1] && ops->eo[1] == ops->eo[2] &&
-                !force_simt_axes) {
+            if (nt == 1 && nx == ny && ny == nz && ops->eo[0] == ops->eo[1] && ops->eo[1] == ops->eo[2]) {
                 AxisDmmaFn f[3];
                 size_t smem = 0;
                 const bool eo2 = ops->eo2 && nx == 128;
@@ -657,7 +655,7 @@ struct scft_solver_s {
         } else {
             // large cubic grids, FP32 precision form: 3xTF32 axis passes
             if (nt == 1 && nx == ny && ny == nz && ops->eo_f32[0] == ops->eo_f32[1] &&
-                ops->eo_f32[1] == ops->eo_f32[2] && !force_simt_axes) {
+                ops->eo_f32[1] == ops->eo_f32[2]) {
                 AxisTf32Fn f[3];
                 size_t smem = 0, stride = 0;
                 for (int ax = 0; ax < 3; ++ax) f[ax] = axis_tf32_kernel_for(nx, ops->eo_f32[ax], ax, &smem, &stride);
