@@ -72,6 +72,12 @@ struct ContourArgs {
     // Boltzmann factors of blocks A and B as (z, y, x) with box (nz, 1, nx)
     alignas(64) CUtensorMap tm_qs[2];
     alignas(64) CUtensorMap tm_ws[2];
+    // two-level kernel: Boltzmann and staging tiles in 8-column panels ([z / 8][row][z % 8],
+    // rows y in plane tiles, x in slab tiles), [0] plane and [1] slab view; contour store of
+    // each chain as (z % 8, row, z / 8, tile, slot), Boltzmann factors of blocks A and B
+    // as (z % 8, row, z / 8, tile)
+    alignas(64) CUtensorMap tm_pq[2][2];
+    alignas(64) CUtensorMap tm_pw[2][2];
 };
 
 __device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
@@ -467,17 +473,42 @@ __device__ __forceinline__ void row_op_ct(const double* __restrict__ F, double* 
 // Where col_op_ct writes its result G[i][c]: kToSmem, a shared-memory slab (row stride LF);
 // kToGlobal, the global exchange buffer (row stride gs), straight from the MMA
 // accumulators, so the stores overlap the other warps' tiles.
-enum ColEpilogue { kToSmem = 0, kToGlobal = 1 };
+// kFinish (two-level kernel): the result y finishes a contour step: q = y W0 goes to the
+// panel staging tile qs (stored from there by TMA) and, if start, q W1 to the slab G.
+enum ColEpilogue { kToSmem = 0, kToGlobal = 1, kFinish = 2 };
 
 struct ColOut {
     double* G;
     long long gs;  // kToGlobal: row stride of G
+    const double* w0 = nullptr;  // kFinish: Boltzmann tiles of the finished / next step (panels)
+    const double* w1 = nullptr;
+    double* qs = nullptr;        // kFinish: staging tile of q (panels)
+    int start = 0;               // kFinish: a next step follows
 };
 
-template <int LF, int EPI>
+// element (i, c) of a tile with PR rows stored in 8-column panels
+template <int PR>
+__device__ __forceinline__ int panel_index(int i, int c) {
+    return ((c >> 3) * PR + i) * 8 + (c & 7);
+}
+
+template <int LF, int EPI, int PR = 0>
 __device__ __forceinline__ void col_store(const ColOut& o, int i, int c, double v0, double v1) {
-    if (EPI == kToSmem) *reinterpret_cast<double2*>(o.G + i * LF + c) = make_double2(v0, v1);
-    else *reinterpret_cast<double2*>(o.G + i * o.gs + c) = make_double2(v0, v1);
+    if constexpr (EPI == kToSmem) {
+        *reinterpret_cast<double2*>(o.G + i * LF + c) = make_double2(v0, v1);
+    } else if constexpr (EPI == kToGlobal) {
+        *reinterpret_cast<double2*>(o.G + i * o.gs + c) = make_double2(v0, v1);
+    } else {
+        const int pi = panel_index<PR>(i, c);
+        const double2 w0 = *reinterpret_cast<const double2*>(o.w0 + pi);
+        v0 = v0 * w0.x;
+        v1 = v1 * w0.y;
+        *reinterpret_cast<double2*>(o.qs + pi) = make_double2(v0, v1);
+        if (o.start) {
+            const double2 w1 = *reinterpret_cast<const double2*>(o.w1 + pi);
+            *reinterpret_cast<double2*>(o.G + i * LF + c) = make_double2(v0 * w1.x, v1 * w1.y);
+        }
+    }
 }
 
 // G[i][c] = sum_j A[i][j] F[j][c] on an R x C slab (leading dimension LF); EPI selects
@@ -677,10 +708,10 @@ __device__ __forceinline__ void col_op_eo2(const double* __restrict__ F, const C
         const int c = cb * 16 + b * 8 + 2 * t;
         const double p10 = pe[b][0] + po[b][0], p11 = pe[b][1] + po[b][1];
         const double p20 = pe[b][0] - po[b][0], p21 = pe[b][1] - po[b][1];
-        col_store<LF, EPI>(out, ip, c, p10 + rA[b][0], p11 + rA[b][1]);
-        col_store<LF, EPI>(out, R - 1 - ip, c, p10 - rA[b][0], p11 - rA[b][1]);
-        col_store<LF, EPI>(out, S::H - 1 - ip, c, p20 + rB[b][0], p21 + rB[b][1]);
-        col_store<LF, EPI>(out, S::H + ip, c, p20 - rB[b][0], p21 - rB[b][1]);
+        col_store<LF, EPI, R>(out, ip, c, p10 + rA[b][0], p11 + rA[b][1]);
+        col_store<LF, EPI, R>(out, R - 1 - ip, c, p10 - rA[b][0], p11 - rA[b][1]);
+        col_store<LF, EPI, R>(out, S::H - 1 - ip, c, p20 + rB[b][0], p21 + rB[b][1]);
+        col_store<LF, EPI, R>(out, S::H + ip, c, p20 - rB[b][0], p21 - rB[b][1]);
     }
 }
 
@@ -852,6 +883,21 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
         ::"r"(smem_u32(dst)), "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
         : "memory");
 }
+// tiled TMA: the 4-D box at (c0, c1, c2, c3) into shared memory, completing on `bar`
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                            unsigned long long* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
+        ::"r"(smem_u32(dst)), "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+        : "memory");
+}
+// tiled TMA: shared memory to the 5-D box at (c0, .., c4), tracked by bulk groups
+__device__ __forceinline__ void tma_store_5d(const CUtensorMap* map, const void* src, int c0, int c1, int c2, int c3,
+                                             int c4) {
+    asm volatile("cp.async.bulk.tensor.5d.global.shared::cta.tile.bulk_group [%0, {%2, %3, %4, %5, %6}], [%1];"
+                 ::"l"(map), "r"(smem_u32(src)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4)
+                 : "memory");
+}
 // tiled TMA: shared memory to the 4-D box at (c0, c1, c2, c3), tracked by bulk groups
 __device__ __forceinline__ void tma_store_4d(const CUtensorMap* map, const void* src, int c0, int c1, int c2, int c3) {
     asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group [%0, {%2, %3, %4, %5}], [%1];"
@@ -881,6 +927,22 @@ __device__ __forceinline__ void tile_scale(double* T, const double* W) {
         const int r = e / PER_ROW, c = (e - r * PER_ROW) * 2;
         double2 v = *reinterpret_cast<double2*>(T + r * LF + c);
         const double2 w = *reinterpret_cast<const double2*>(W + r * N + c);
+        v.x = v.x * w.x;
+        v.y = v.y * w.y;
+        *reinterpret_cast<double2*>(T + r * LF + c) = v;
+    }
+}
+
+// T <- T * W (T row stride LF, W in 8-column panels)
+template <int N, int LF>
+__device__ __forceinline__ void tile_scale_panel(double* T, const double* W) {
+    constexpr int PER_ROW = N / 2;
+    constexpr int TOTAL = N * PER_ROW;
+#pragma unroll 4
+    for (int e = threadIdx.x; e < TOTAL; e += kContourThreads) {
+        const int r = e / PER_ROW, c = (e - r * PER_ROW) * 2;
+        double2 v = *reinterpret_cast<double2*>(T + r * LF + c);
+        const double2 w = *reinterpret_cast<const double2*>(W + panel_index<N>(r, c));
         v.x = v.x * w.x;
         v.y = v.y * w.y;
         *reinterpret_cast<double2*>(T + r * LF + c) = v;
@@ -1000,7 +1062,8 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
     const int warp = threadIdx.x >> 5;
     {
         const void* tiles[3] = {W0, W1, QS};
-        const int e = tma_alignment_error(tiles, 3, a.tm_qs, 2) | tma_alignment_error(tiles, 0, a.tm_ws, 2);
+        const int e = tma_alignment_error(tiles, 3, a.tm_qs, 2) | tma_alignment_error(tiles, 0, a.tm_ws, 2) |
+                      tma_alignment_error(tiles, 0, &a.tm_pq[0][0], 4) | tma_alignment_error(tiles, 0, &a.tm_pw[0][0], 4);
         if (e) {
             if (threadIdx.x == 0) atomicOr(a.error, e);
             return;
@@ -1040,8 +1103,15 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
         const unsigned bytes = ((k >= 1) + (k < U)) * TILE_BYTES;
         if ((threadIdx.x & 31) == 0) mbar_expect_tx(&s_bar, bytes);
         __syncwarp();
-        if (k >= 1) bulk_tile_load<double, N>(W0, a.wds[blk_of(k - 1)], p, plane, &a.tm_ws[blk_of(k - 1)], &s_bar);
-        if (k < U) bulk_tile_load<double, N>(W1, a.wds[blk_of(k)], p, plane, &a.tm_ws[blk_of(k)], &s_bar);
+        if constexpr (EO2) {  // 8-column panels, the layout the finishing epilogue reads
+            if ((threadIdx.x & 31) == 0) {
+                if (k >= 1) tma_load_4d(W0, &a.tm_pw[blk_of(k - 1)][plane ? 0 : 1], 0, 0, 0, p, &s_bar);
+                if (k < U) tma_load_4d(W1, &a.tm_pw[blk_of(k)][plane ? 0 : 1], 0, 0, 0, p, &s_bar);
+            }
+        } else {
+            if (k >= 1) bulk_tile_load<double, N>(W0, a.wds[blk_of(k - 1)], p, plane, &a.tm_ws[blk_of(k - 1)], &s_bar);
+            if (k < U) bulk_tile_load<double, N>(W1, a.wds[blk_of(k)], p, plane, &a.tm_ws[blk_of(k)], &s_bar);
+        }
     };
     unsigned wpar = 0;  // parity of the pending W phase of s_bar
     // error exit: let this block's bulk copies finish (bounded), then return
@@ -1103,7 +1173,38 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
         }
         double* cur = T0;
         double* oth = T1;
-        if (k >= 1) {
+        if (EO2 && k >= 1) {
+            // finish step k-1: the axis ops this layout owns; the last one's epilogue applies
+            // D, writes q(s+1) to the panel staging tile and D q(s+1) to the work tile
+            if (plane) row_z(cur, oth);
+            if (warp == 0) bulk_wait_read();  // the previous q store has left QS
+            if (!mbar_wait(&s_bar, wpar, a.spin_limit)) s_fail = 1;
+            __syncthreads();
+            if (s_fail) {
+                if (threadIdx.x == 0) atomicOr(a.error, 2);
+                drain(true);
+                return;
+            }
+            wpar ^= 1u;
+            ColOut fo{plane ? cur : oth, 0};
+            fo.w0 = W0;
+            fo.w1 = W1;
+            fo.qs = QS;
+            fo.start = k < U;
+            if constexpr (EO2) col_op_eo2<N, N, LF, kFinish>(plane ? oth : cur, fo, sops + (plane ? OFFY : 0));
+            if (!plane) {
+                double* tmp = cur;
+                cur = oth;
+                oth = tmp;
+            }
+            fence_async_smem();
+            __syncthreads();
+            if (warp == 0 && threadIdx.x == 0) {
+                tma_store_5d(&a.tm_pq[c][plane ? 0 : 1], QS, 0, 0, 0, p, (int)(slot0 + (long long)dir * k));
+                bulk_commit();
+            }
+        }
+        if (!EO2 && k >= 1) {
             // finish step k-1: the axis ops this layout owns, then D, q(s+1) to the staging tile
             if (plane) {
                 row_z(cur, oth);
@@ -1117,24 +1218,28 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
             }
             if (warp == 0) bulk_wait_read();  // the previous q store has left QS
         }
-        if (!mbar_wait(&s_bar, wpar, a.spin_limit)) s_fail = 1;
-        __syncthreads();
-        if (s_fail) {  // every thread leaves here: the W load still lands in this block's memory first
-            if (threadIdx.x == 0) atomicOr(a.error, 2);
-            drain(true);
-            return;
-        }
-        wpar ^= 1u;
-        if (k >= 1) {
-            // a separate pass: the dense TMA tiles (row stride n) would bank-conflict with the
-            // MMA fragment pattern of an epilogue
-            tile_finish<N, LF>(cur, W0, W1, QS, k < U);
-            fence_async_smem();
+        if (!EO2 || k == 0) {
+            if (!mbar_wait(&s_bar, wpar, a.spin_limit)) s_fail = 1;
             __syncthreads();
-            if (warp == 0) bulk_tile_store<double, N>(q, QS, p, slot0 + (long long)dir * k, plane, &a.tm_qs[c]);
-        } else {
-            tile_scale<N, LF>(cur, W1);
-            __syncthreads();
+            if (s_fail) {  // every thread leaves here: the W load still lands in this block's memory first
+                if (threadIdx.x == 0) atomicOr(a.error, 2);
+                drain(true);
+                return;
+            }
+            wpar ^= 1u;
+            if (k >= 1) {
+                // one level: a separate pass, the dense TMA tiles (row stride n) would
+                // bank-conflict with the MMA fragment pattern of an epilogue (the two-level
+                // kernel's panel tiles do not, and it finishes in the epilogue above)
+                tile_finish<N, LF>(cur, W0, W1, QS, k < U);
+                fence_async_smem();
+                __syncthreads();
+                if (warp == 0) bulk_tile_store<double, N>(q, QS, p, slot0 + (long long)dir * k, plane, &a.tm_qs[c]);
+            } else {
+                if constexpr (EO2) tile_scale_panel<N, LF>(cur, W1);
+                else tile_scale<N, LF>(cur, W1);
+                __syncthreads();
+            }
         }
         if (k < U) {
             if (warp == 0) issue_w(k + 1);  // W0/W1 are free: prefetch the next phase's factors
