@@ -168,12 +168,29 @@ __device__ __forceinline__ void row_op_f32(const float* __restrict__ F, float* _
 struct ColOutF {
     float* G;
     long long gs;
+    const float* w0 = nullptr;  // kFinish: Boltzmann tiles of the finished / next step (panels)
+    const float* w1 = nullptr;
+    float* qs = nullptr;        // kFinish: staging tile of q (panels)
+    int start = 0;              // kFinish: a next step follows
 };
 
-template <int LF, int EPI>
+template <int LF, int EPI, int PR = 0>
 __device__ __forceinline__ void col_store_f32(const ColOutF& o, int i, int c, float v0, float v1) {
-    if (EPI == kToSmem) *reinterpret_cast<float2*>(o.G + i * LF + c) = make_float2(v0, v1);
-    else *reinterpret_cast<float2*>(o.G + i * o.gs + c) = make_float2(v0, v1);
+    if constexpr (EPI == kToSmem) {
+        *reinterpret_cast<float2*>(o.G + i * LF + c) = make_float2(v0, v1);
+    } else if constexpr (EPI == kToGlobal) {
+        *reinterpret_cast<float2*>(o.G + i * o.gs + c) = make_float2(v0, v1);
+    } else {  // kFinish, as col_store
+        const int pi = panel_index<PR>(i, c);
+        const float2 w0 = *reinterpret_cast<const float2*>(o.w0 + pi);
+        v0 = v0 * w0.x;
+        v1 = v1 * w0.y;
+        *reinterpret_cast<float2*>(o.qs + pi) = make_float2(v0, v1);
+        if (o.start) {
+            const float2 w1 = *reinterpret_cast<const float2*>(o.w1 + pi);
+            *reinterpret_cast<float2*>(o.G + i * LF + c) = make_float2(v0 * w1.x, v1 * w1.y);
+        }
+    }
 }
 
 // G[i][c] = sum_j A[i][j] F[j][c] on an R x C slab: m16 tiles over i, n8 tiles over c
@@ -243,10 +260,10 @@ __device__ __forceinline__ void col_op_f32(const float* __restrict__ F, const Co
                 const float p0 = dP[b][2 * h], p1 = dP[b][2 * h + 1];
                 if (EO) {
                     const float r0 = dR[b][2 * h], r1 = dR[b][2 * h + 1];
-                    col_store_f32<LF, EPI>(out, i, c, p0 + r0, p1 + r1);
-                    col_store_f32<LF, EPI>(out, R - 1 - i, c, p0 - r0, p1 - r1);
+                    col_store_f32<LF, EPI, R>(out, i, c, p0 + r0, p1 + r1);
+                    col_store_f32<LF, EPI, R>(out, R - 1 - i, c, p0 - r0, p1 - r1);
                 } else {
-                    col_store_f32<LF, EPI>(out, i, c, p0, p1);
+                    col_store_f32<LF, EPI, R>(out, i, c, p0, p1);
                 }
             }
         }
@@ -273,7 +290,7 @@ __device__ __forceinline__ void tile_fetch_f32(float* sm, const float* gm, long 
     }
 }
 
-// T <- T * W (T row stride LF, W dense N x N)
+// T <- T * W (T row stride LF, W in 8-column panels)
 template <int N, int LF>
 __device__ __forceinline__ void tile_scale_f32(float* T, const float* W) {
     constexpr int PER_ROW = N / 4;
@@ -282,7 +299,7 @@ __device__ __forceinline__ void tile_scale_f32(float* T, const float* W) {
     for (int e = threadIdx.x; e < TOTAL; e += kContourThreads) {
         const int r = e / PER_ROW, c = (e - r * PER_ROW) * 4;
         float4 v = *reinterpret_cast<float4*>(T + r * LF + c);
-        const float4 w = *reinterpret_cast<const float4*>(W + r * N + c);
+        const float4 w = *reinterpret_cast<const float4*>(W + panel_index<N>(r, c));
         v.x *= w.x;
         v.y *= w.y;
         v.z *= w.z;
@@ -290,36 +307,10 @@ __device__ __forceinline__ void tile_scale_f32(float* T, const float* W) {
         *reinterpret_cast<float4*>(T + r * LF + c) = v;
     }
 }
-// v = T * W0 into the dense staging tile QS (stored by the bulk-copy engine); if start,
-// T <- v * W1 (D of the next step)
-template <int N, int LF>
-__device__ __forceinline__ void tile_finish_f32(float* T, const float* W0, const float* W1, float* QS, bool start) {
-    constexpr int PER_ROW = N / 4;
-    constexpr int TOTAL = N * PER_ROW;
-#pragma unroll 4
-    for (int e = threadIdx.x; e < TOTAL; e += kContourThreads) {
-        const int r = e / PER_ROW, c = (e - r * PER_ROW) * 4;
-        float4 v = *reinterpret_cast<float4*>(T + r * LF + c);
-        const float4 w0 = *reinterpret_cast<const float4*>(W0 + r * N + c);
-        v.x *= w0.x;
-        v.y *= w0.y;
-        v.z *= w0.z;
-        v.w *= w0.w;
-        *reinterpret_cast<float4*>(QS + r * N + c) = v;
-        if (start) {
-            const float4 w1 = *reinterpret_cast<const float4*>(W1 + r * N + c);
-            v.x *= w1.x;
-            v.y *= w1.y;
-            v.z *= w1.z;
-            v.w *= w1.w;
-            *reinterpret_cast<float4*>(T + r * LF + c) = v;
-        }
-    }
-}
 
 // Shared memory: operators, two padded work tiles, the four Boltzmann-factor tiles of
-// this block's unit (blocks A and B, plane and slab layout; loaded once per launch),
-// and the dense q staging tile.
+// this block's unit (blocks A and B, plane and slab layout; loaded once per launch by
+// TMA) and the q staging tile, both in 8-column panels (the finishing epilogue's layout).
 template <int N, bool EO>
 struct AltShapeF {
     static constexpr int LF = N + 4;
@@ -344,8 +335,8 @@ struct ContourArgsF {
     int* error;
     long long spin_limit;
     unsigned* flags;       // [chain][plane|slab][consumer][producer], zeroed by the host
-    alignas(64) CUtensorMap tm_qs[2];  // slab-layout TMA boxes, as in ContourArgs
-    alignas(64) CUtensorMap tm_ws[2];
+    alignas(64) CUtensorMap tm_pq[2][2];  // panel tiles, as ContourArgs::tm_pq / tm_pw
+    alignas(64) CUtensorMap tm_pw[2][2];
 };
 
 template <int N, bool EO>
@@ -394,7 +385,7 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel_f32(con
     const int U = a.t_end;
     {
         const void* tiles[6] = {WP, WP + S::WT, WS, WS + S::WT, QS, T0};
-        const int e = tma_alignment_error(tiles, 5, a.tm_qs, 2) | tma_alignment_error(tiles, 0, a.tm_ws, 2);
+        const int e = tma_alignment_error(tiles, 5, &a.tm_pq[0][0], 4) | tma_alignment_error(tiles, 0, &a.tm_pw[0][0], 4);
         if (e) {
             if (threadIdx.x == 0) atomicOr(a.error, e);
             return;
@@ -411,10 +402,11 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel_f32(con
         // the unit's Boltzmann factors of both blocks in both layouts, once per launch
         if ((threadIdx.x & 31) == 0) mbar_expect_tx(&s_bar, 4 * TILE_BYTES);
         __syncwarp();
-        for (int b = 0; b < 2; ++b) {
-            bulk_tile_load<float, N>(WP + b * S::WT, a.wds[b], p, true, &a.tm_ws[b], &s_bar);
-            bulk_tile_load<float, N>(WS + b * S::WT, a.wds[b], p, false, &a.tm_ws[b], &s_bar);
-        }
+        if ((threadIdx.x & 31) == 0)  // in 8-column panels, the layout the finishing epilogue reads
+            for (int b = 0; b < 2; ++b) {
+                tma_load_4d(WP + b * S::WT, &a.tm_pw[b][0], 0, 0, 0, p, &s_bar);
+                tma_load_4d(WS + b * S::WT, &a.tm_pw[b][1], 0, 0, 0, p, &s_bar);
+            }
     }
     op_copy_async(sops, a.ops, S::OPS);
     cp_async_wait_all();
@@ -472,26 +464,28 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel_f32(con
         float* cur = T0;
         float* oth = T1;
         if (k >= 1) {
-            if (plane) {
-                row_op_f32<N, N, LF, EO>(cur, oth, sops + OFFZ);
-                __syncthreads();
-                col_op_f32<N, N, LF, EO>(oth, cur, sops + OFFY);
-            } else {
-                col_op_f32<N, N, LF, EO>(cur, oth, sops);
+            // finish step k-1: the axis ops this layout owns; the last one's epilogue applies
+            // D, writes q(s+1) to the panel staging tile and D q(s+1) to the work tile
+            if (plane) row_op_f32<N, N, LF, EO>(cur, oth, sops + OFFZ);
+            if (warp == 0) bulk_wait_read();  // the previous q store has left QS
+            __syncthreads();
+            ColOutF fo{plane ? cur : oth, 0};
+            fo.w0 = Wl + blk_of(k - 1) * S::WT;
+            fo.w1 = Wl + (k < U ? blk_of(k) : 0) * S::WT;
+            fo.qs = QS;
+            fo.start = k < U;
+            col_op_f32<N, N, LF, EO, kFinish>(plane ? oth : cur, fo, sops + (plane ? OFFY : 0));
+            if (!plane) {
                 float* tmp = cur;
                 cur = oth;
                 oth = tmp;
             }
-            if (warp == 0) bulk_wait_read();  // the previous q store has left QS
-            __syncthreads();
-            // a separate pass: the dense TMA tiles (row stride n) would bank-conflict with the
-            // MMA fragment pattern of an epilogue
-            const float* W0 = Wl + blk_of(k - 1) * S::WT;
-            const float* W1 = Wl + (k < U ? blk_of(k) : 0) * S::WT;
-            tile_finish_f32<N, LF>(cur, W0, W1, QS, k < U);
             fence_async_smem();
             __syncthreads();
-            if (warp == 0) bulk_tile_store<float, N>(q, QS, p, slot0 + (long long)dir * k, plane, &a.tm_qs[c]);
+            if (threadIdx.x == 0) {
+                tma_store_5d(&a.tm_pq[c][plane ? 0 : 1], QS, 0, 0, 0, p, (int)(slot0 + (long long)dir * k));
+                bulk_commit();
+            }
         } else {
             tile_scale_f32<N, LF>(cur, Wl + blk_of(0) * S::WT);
             __syncthreads();

@@ -89,17 +89,18 @@ int encode_slab_map(CUtensorMap* m, const void* base, int n, long long slots, bo
 // tiles in 8-column panels: dims (z % 8, row, z / 8, tile[, slot]), box (8, n, n / 8, 1[, 1]),
 // so a box lands in shared memory as [z / 8][row][z % 8].  plane: row = y, tile = x;
 // else (slab): row = x, tile = y.
-int encode_panel_map(CUtensorMap* m, const void* base, int n, long long slots, bool plane) {
+int encode_panel_map(CUtensorMap* m, const void* base, int n, long long slots, bool plane, bool fp64 = true) {
     PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
     if (!enc) return fail(SCFT_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
     if (reinterpret_cast<uintptr_t>(base) % 16) return fail(SCFT_ERR_INVALID_ARG, "TMA base not 16-byte aligned");
     if (n % 8 || n > 256) return fail(SCFT_ERR_INVALID_ARG, "panel tiles need n a multiple of 8, at most 256");
-    const cuuint64_t es = 8, N = (cuuint64_t)n;
+    const cuuint64_t es = fp64 ? 8 : 4, N = (cuuint64_t)n;
     cuuint64_t dims[5] = {8, N, N / 8, N, (cuuint64_t)(slots > 0 ? slots : 1)};
     cuuint64_t strides[4] = {plane ? N * es : N * N * es, 8 * es, plane ? N * N * es : N * es, N * N * N * es};
     cuuint32_t box[5] = {8u, (cuuint32_t)n, (cuuint32_t)(n / 8), 1u, 1u};
     cuuint32_t estr[5] = {1u, 1u, 1u, 1u, 1u};
-    const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, slots > 0 ? 5u : 4u, const_cast<void*>(base), dims,
+    const CUresult r = enc(m, fp64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                           slots > 0 ? 5u : 4u, const_cast<void*>(base), dims,
                            strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                            CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS)
@@ -860,10 +861,12 @@ struct scft_diblock_s {
         a.spin_limit = spin_limit;
         a.flags = flags.p;
         const int n = (int)solver->grid_phy[0];
-        CKR(encode_slab_map(&a.tm_qs[0], q, n, (long long)U + 1, false));
-        CKR(encode_slab_map(&a.tm_qs[1], qc, n, (long long)U + 1, false));
-        CKR(encode_slab_map(&a.tm_ws[0], wAds, n, 0, false));
-        CKR(encode_slab_map(&a.tm_ws[1], wBds, n, 0, false));
+        for (int v = 0; v < 2; ++v) {  // panel tiles, plane [0] and slab [1] views
+            CKR(encode_panel_map(&a.tm_pq[0][v], q, n, (long long)U + 1, v == 0, false));
+            CKR(encode_panel_map(&a.tm_pq[1][v], qc, n, (long long)U + 1, v == 0, false));
+            CKR(encode_panel_map(&a.tm_pw[0][v], wAds, n, 0, v == 0, false));
+            CKR(encode_panel_map(&a.tm_pw[1][v], wBds, n, 0, v == 0, false));
+        }
         CK(cudaMemsetAsync(flags.p, 0, flags.n * sizeof(unsigned), st));
         cudaLaunchConfig_t cfg{};
         cfg.gridDim = dim3((unsigned)persistent_grid);
