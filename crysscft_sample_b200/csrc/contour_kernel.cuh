@@ -67,12 +67,7 @@ struct ContourArgs {
     int* error;             // bit 0: barrier wait gave up
     long long spin_limit;
     unsigned* flags;        // alternating kernel: [chain][plane|slab][consumer][producer] last finished phase + 1, zeroed by the host
-    // alternating kernel: TMA descriptors of the slab-layout tiles (an nx x nz tile at fixed y):
-    // the contour store of each chain as (z, y, x, slot) with box (nz, 1, nx, 1), and the
-    // Boltzmann factors of blocks A and B as (z, y, x) with box (nz, 1, nx)
-    alignas(64) CUtensorMap tm_qs[2];
-    alignas(64) CUtensorMap tm_ws[2];
-    // two-level kernel: Boltzmann and staging tiles in 8-column panels ([z / 8][row][z % 8],
+    // alternating kernel: Boltzmann and staging tiles in 8-column panels ([z / 8][row][z % 8],
     // rows y in plane tiles, x in slab tiles), [0] plane and [1] slab view; contour store of
     // each chain as (z % 8, row, z / 8, tile, slot), Boltzmann factors of blocks A and B
     // as (z % 8, row, z / 8, tile)
@@ -575,10 +570,10 @@ __device__ __forceinline__ void col_op_ct(const double* __restrict__ F, const Co
                 const int i = (mb + a) * 8 + g;
                 const int c = (nb + b) * 8 + 2 * t;
                 if (EO) {
-                    col_store<LF, EPI>(out, i, c, dP[a][b][0] + dR[a][b][0], dP[a][b][1] + dR[a][b][1]);
-                    col_store<LF, EPI>(out, R - 1 - i, c, dP[a][b][0] - dR[a][b][0], dP[a][b][1] - dR[a][b][1]);
+                    col_store<LF, EPI, R>(out, i, c, dP[a][b][0] + dR[a][b][0], dP[a][b][1] + dR[a][b][1]);
+                    col_store<LF, EPI, R>(out, R - 1 - i, c, dP[a][b][0] - dR[a][b][0], dP[a][b][1] - dR[a][b][1]);
                 } else {
-                    col_store<LF, EPI>(out, i, c, dP[a][b][0], dP[a][b][1]);
+                    col_store<LF, EPI, R>(out, i, c, dP[a][b][0], dP[a][b][1]);
                 }
             }
     }
@@ -823,12 +818,13 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_kernel_ct(const Co
 // Phase k (k = 0..U) finishes step k-1 (k >= 1) and starts step k (k < U); plane
 // phases have even k.  One exchange per step and no grid barrier: a unit waits only for
 // the release flags of the units whose rows it reads.  The Boltzmann-factor tiles of the
-// next phase are loaded by TMA as soon as the current ones are consumed, and finished
-// q(s) tiles leave by TMA stores, so neither sits on the critical path.
+// next phase are loaded by TMA as soon as the current ones are consumed; the last axis
+// operation of a phase applies D in its epilogue and finished q(s) tiles leave by TMA
+// stores, so neither sits on the critical path.
 // ---------------------------------------------------------------------------
 namespace crysscft {
 
-// ---- bulk-copy engine (cp.async.bulk, no tensor map) and mbarriers ----------------
+// ---- TMA (cp.async.bulk.tensor) and mbarriers ---------------------------------------
 __device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
@@ -857,32 +853,12 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
     }
     return true;
 }
-// global -> shared bulk copy (16-byte aligned, size a multiple of 16) completing on `bar`
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
-// shared -> global bulk copy, tracked by the issuing thread's bulk groups
-__device__ __forceinline__ void bulk_store(void* dst, const void* src, unsigned bytes) {
-    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)),
-                 "r"(bytes)
-                 : "memory");
-}
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 // the source shared memory of this thread's bulk stores may be overwritten after this
 __device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 // generic-proxy shared-memory writes become visible to the bulk-copy engine
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-// tiled TMA: 3-D box at (c0, c1, c2) into shared memory, completing on `bar`
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1, int c2,
-                                            unsigned long long* bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
-        ::"r"(smem_u32(dst)), "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
-        : "memory");
-}
 // tiled TMA: the 4-D box at (c0, c1, c2, c3) into shared memory, completing on `bar`
 __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
                                             unsigned long long* bar) {
@@ -898,13 +874,6 @@ __device__ __forceinline__ void tma_store_5d(const CUtensorMap* map, const void*
                  ::"l"(map), "r"(smem_u32(src)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4)
                  : "memory");
 }
-// tiled TMA: shared memory to the 4-D box at (c0, c1, c2, c3), tracked by bulk groups
-__device__ __forceinline__ void tma_store_4d(const CUtensorMap* map, const void* src, int c0, int c1, int c2, int c3) {
-    asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group [%0, {%2, %3, %4, %5}], [%1];"
-                 ::"l"(map), "r"(smem_u32(src)), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
-                 : "memory");
-}
-
 // N x N tile from global (row stride gs) into shared memory (row stride LF) with cp.async
 template <int N, int LF>
 __device__ __forceinline__ void tile_fetch(double* sm, const double* gm, long long gs) {
@@ -914,22 +883,6 @@ __device__ __forceinline__ void tile_fetch(double* sm, const double* gm, long lo
     for (int e = threadIdx.x; e < TOTAL; e += kContourThreads) {
         const int r = e / PER_ROW, c = (e - r * PER_ROW) * 2;
         cp_async16(sm + r * LF + c, gm + r * gs + c);
-    }
-}
-
-// T <- T * W (T row stride LF, W dense N x N)
-template <int N, int LF>
-__device__ __forceinline__ void tile_scale(double* T, const double* W) {
-    constexpr int PER_ROW = N / 2;
-    constexpr int TOTAL = N * PER_ROW;
-#pragma unroll 4
-    for (int e = threadIdx.x; e < TOTAL; e += kContourThreads) {
-        const int r = e / PER_ROW, c = (e - r * PER_ROW) * 2;
-        double2 v = *reinterpret_cast<double2*>(T + r * LF + c);
-        const double2 w = *reinterpret_cast<const double2*>(W + r * N + c);
-        v.x = v.x * w.x;
-        v.y = v.y * w.y;
-        *reinterpret_cast<double2*>(T + r * LF + c) = v;
     }
 }
 
@@ -949,32 +902,11 @@ __device__ __forceinline__ void tile_scale_panel(double* T, const double* W) {
     }
 }
 
-// v = T * W0 into the dense staging tile QS (the finished q(s+1), stored from there by
-// the bulk-copy engine); if start, T <- v * W1 (D of the next step)
-template <int N, int LF>
-__device__ __forceinline__ void tile_finish(double* T, const double* W0, const double* W1, double* QS, bool start) {
-    constexpr int PER_ROW = N / 2;
-    constexpr int TOTAL = N * PER_ROW;
-#pragma unroll 4
-    for (int e = threadIdx.x; e < TOTAL; e += kContourThreads) {
-        const int r = e / PER_ROW, c = (e - r * PER_ROW) * 2;
-        double2 v = *reinterpret_cast<double2*>(T + r * LF + c);
-        const double2 w0 = *reinterpret_cast<const double2*>(W0 + r * N + c);
-        v.x = v.x * w0.x;
-        v.y = v.y * w0.y;
-        *reinterpret_cast<double2*>(QS + r * N + c) = v;
-        if (start) {
-            const double2 w1 = *reinterpret_cast<const double2*>(W1 + r * N + c);
-            v.x = v.x * w1.x;
-            v.y = v.y * w1.y;
-            *reinterpret_cast<double2*>(T + r * LF + c) = v;
-        }
-    }
-}
-
 // Shared-memory carve-up of the alternating kernel: operators, two padded work tiles
-// (row stride LF, conflict-free MMA fragments), and three dense N x N tiles filled and
-// drained by the bulk-copy engine (Boltzmann factors W0/W1, q staging tile QS).
+// (row stride LF, conflict-free MMA fragments), and three N x N tiles in 8-column panels
+// filled and drained by TMA (Boltzmann factors W0/W1, q staging tile QS); the last axis
+// operation of a phase reads and writes the panels from its MMA accumulators, where two
+// rows x 8 columns per quarter-warp fall on distinct banks.
 template <int N, bool EO, bool EO2 = false>
 struct AltShape {
     static constexpr int LF = N + 4;
@@ -1002,29 +934,6 @@ __device__ __forceinline__ int tma_alignment_error(const void* const* tiles, int
     for (int i = 0; i < nmaps; ++i)
         if (reinterpret_cast<uintptr_t>(&maps[i]) & 63u) e |= 16;
     return e;
-}
-
-// Lane 0 of warp 0 loads one N x N Boltzmann-factor tile: a plane (contiguous, one bulk
-// copy) or a slab (N rows of stride N^2: one tiled TMA box through `slab_map`).
-template <typename T, int N>
-__device__ __forceinline__ void bulk_tile_load(T* dst, const T* src, int p, bool plane, const CUtensorMap* slab_map,
-                                               unsigned long long* bar) {
-    if ((threadIdx.x & 31) != 0) return;
-    if (plane) bulk_load(dst, src + (long long)p * N * N, (unsigned)(N * N * sizeof(T)), bar);
-    else tma_load_3d(dst, slab_map, 0, p, 0, bar);
-}
-
-// Lane 0 of warp 0 stores the dense staging tile QS to contour slot `slot`: a plane
-// (contiguous, one bulk copy) or a slab (one tiled TMA box through `slab_map`), and
-// commits it as one bulk group.
-template <typename T, int N>
-__device__ __forceinline__ void bulk_tile_store(T* q, const T* QS, int p, long long slot, bool plane,
-                                                const CUtensorMap* slab_map) {
-    if ((threadIdx.x & 31) != 0) return;
-    constexpr long long M = (long long)N * N * N;
-    if (plane) bulk_store(q + slot * M + (long long)p * N * N, QS, (unsigned)(N * N * sizeof(T)));
-    else tma_store_4d(slab_map, QS, 0, p, 0, (int)slot);
-    bulk_commit();
 }
 
 template <int N, bool EO, bool EO2 = false>
@@ -1062,8 +971,7 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
     const int warp = threadIdx.x >> 5;
     {
         const void* tiles[3] = {W0, W1, QS};
-        const int e = tma_alignment_error(tiles, 3, a.tm_qs, 2) | tma_alignment_error(tiles, 0, a.tm_ws, 2) |
-                      tma_alignment_error(tiles, 0, &a.tm_pq[0][0], 4) | tma_alignment_error(tiles, 0, &a.tm_pw[0][0], 4);
+        const int e = tma_alignment_error(tiles, 3, &a.tm_pq[0][0], 4) | tma_alignment_error(tiles, 0, &a.tm_pw[0][0], 4);
         if (e) {
             if (threadIdx.x == 0) atomicOr(a.error, e);
             return;
@@ -1103,14 +1011,9 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
         const unsigned bytes = ((k >= 1) + (k < U)) * TILE_BYTES;
         if ((threadIdx.x & 31) == 0) mbar_expect_tx(&s_bar, bytes);
         __syncwarp();
-        if constexpr (EO2) {  // 8-column panels, the layout the finishing epilogue reads
-            if ((threadIdx.x & 31) == 0) {
-                if (k >= 1) tma_load_4d(W0, &a.tm_pw[blk_of(k - 1)][plane ? 0 : 1], 0, 0, 0, p, &s_bar);
-                if (k < U) tma_load_4d(W1, &a.tm_pw[blk_of(k)][plane ? 0 : 1], 0, 0, 0, p, &s_bar);
-            }
-        } else {
-            if (k >= 1) bulk_tile_load<double, N>(W0, a.wds[blk_of(k - 1)], p, plane, &a.tm_ws[blk_of(k - 1)], &s_bar);
-            if (k < U) bulk_tile_load<double, N>(W1, a.wds[blk_of(k)], p, plane, &a.tm_ws[blk_of(k)], &s_bar);
+        if ((threadIdx.x & 31) == 0) {  // 8-column panels, the layout the finishing epilogue reads
+            if (k >= 1) tma_load_4d(W0, &a.tm_pw[blk_of(k - 1)][plane ? 0 : 1], 0, 0, 0, p, &s_bar);
+            if (k < U) tma_load_4d(W1, &a.tm_pw[blk_of(k)][plane ? 0 : 1], 0, 0, 0, p, &s_bar);
         }
     };
     unsigned wpar = 0;  // parity of the pending W phase of s_bar
@@ -1173,7 +1076,7 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
         }
         double* cur = T0;
         double* oth = T1;
-        if (EO2 && k >= 1) {
+        if (k >= 1) {
             // finish step k-1: the axis ops this layout owns; the last one's epilogue applies
             // D, writes q(s+1) to the panel staging tile and D q(s+1) to the work tile
             if (plane) row_z(cur, oth);
@@ -1192,6 +1095,7 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
             fo.qs = QS;
             fo.start = k < U;
             if constexpr (EO2) col_op_eo2<N, N, LF, kFinish>(plane ? oth : cur, fo, sops + (plane ? OFFY : 0));
+            else col_op_ct<N, N, LF, EO, kFinish>(plane ? oth : cur, fo, sops + (plane ? OFFY : 0));
             if (!plane) {
                 double* tmp = cur;
                 cur = oth;
@@ -1204,21 +1108,7 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
                 bulk_commit();
             }
         }
-        if (!EO2 && k >= 1) {
-            // finish step k-1: the axis ops this layout owns, then D, q(s+1) to the staging tile
-            if (plane) {
-                row_z(cur, oth);
-                __syncthreads();
-                col_smem(oth, cur, OFFY);
-            } else {
-                col_smem(cur, oth, 0);
-                double* tmp = cur;
-                cur = oth;
-                oth = tmp;
-            }
-            if (warp == 0) bulk_wait_read();  // the previous q store has left QS
-        }
-        if (!EO2 || k == 0) {
+        if (k == 0) {
             if (!mbar_wait(&s_bar, wpar, a.spin_limit)) s_fail = 1;
             __syncthreads();
             if (s_fail) {  // every thread leaves here: the W load still lands in this block's memory first
@@ -1227,19 +1117,8 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
                 return;
             }
             wpar ^= 1u;
-            if (k >= 1) {
-                // one level: a separate pass, the dense TMA tiles (row stride n) would
-                // bank-conflict with the MMA fragment pattern of an epilogue (the two-level
-                // kernel's panel tiles do not, and it finishes in the epilogue above)
-                tile_finish<N, LF>(cur, W0, W1, QS, k < U);
-                fence_async_smem();
-                __syncthreads();
-                if (warp == 0) bulk_tile_store<double, N>(q, QS, p, slot0 + (long long)dir * k, plane, &a.tm_qs[c]);
-            } else {
-                if constexpr (EO2) tile_scale_panel<N, LF>(cur, W1);
-                else tile_scale<N, LF>(cur, W1);
-                __syncthreads();
-            }
+            tile_scale_panel<N, LF>(cur, W1);
+            __syncthreads();
         }
         if (k < U) {
             if (warp == 0) issue_w(k + 1);  // W0/W1 are free: prefetch the next phase's factors

@@ -65,26 +65,6 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     return fn;
 }
 
-// TMA descriptor of the slab-layout tiles of a cubic n^3 field (x, y, z; z fastest): box
-// (z: n, y: 1, x: n) at a fixed y.  slots = 0: one field (rank 3); slots > 0: that many
-// fields back to back, a contour store (rank 4, the slot outermost).
-int encode_slab_map(CUtensorMap* m, const void* base, int n, long long slots, bool fp64) {
-    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
-    if (!enc) return fail(SCFT_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
-    if (reinterpret_cast<uintptr_t>(base) % 16) return fail(SCFT_ERR_INVALID_ARG, "TMA base not 16-byte aligned");
-    const cuuint64_t es = fp64 ? 8 : 4, N = (cuuint64_t)n;
-    cuuint64_t dims[4] = {N, N, N, (cuuint64_t)(slots > 0 ? slots : 1)};
-    cuuint64_t strides[3] = {N * es, N * N * es, N * N * N * es};
-    cuuint32_t box[4] = {(cuuint32_t)n, 1u, (cuuint32_t)n, 1u};
-    cuuint32_t estr[4] = {1u, 1u, 1u, 1u};
-    const CUresult r = enc(m, fp64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
-                           slots > 0 ? 4u : 3u, const_cast<void*>(base), dims, strides, box, estr,
-                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                           CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) return fail(SCFT_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
-    return SCFT_OK;
-}
-
 // Tensor map of an n^3 FP64 field (slots > 0: a contour store of `slots` fields) as n x n
 // tiles in 8-column panels: dims (z % 8, row, z / 8, tile[, slot]), box (8, n, n / 8, 1[, 1]),
 // so a box lands in shared memory as [z / 8][row][z % 8].  plane: row = y, tile = x;
@@ -967,17 +947,11 @@ struct scft_diblock_s {
         CK(cudaMemsetAsync(ctrl.p, 0, sizeof(unsigned), st));
         if (alternating) {
             const int n = (int)solver->grid_phy[0];
-            CKR(encode_slab_map(&a.tm_qs[0], q, n, (long long)U + 1, true));
-            CKR(encode_slab_map(&a.tm_qs[1], qc, n, (long long)U + 1, true));
-            CKR(encode_slab_map(&a.tm_ws[0], wAds, n, 0, true));
-            CKR(encode_slab_map(&a.tm_ws[1], wBds, n, 0, true));
-            if (alt_eo2) {  // the two-level kernel's panel tiles, plane [0] and slab [1] views
-                for (int v = 0; v < 2; ++v) {
-                    CKR(encode_panel_map(&a.tm_pq[0][v], q, n, (long long)U + 1, v == 0));
-                    CKR(encode_panel_map(&a.tm_pq[1][v], qc, n, (long long)U + 1, v == 0));
-                    CKR(encode_panel_map(&a.tm_pw[0][v], wAds, n, 0, v == 0));
-                    CKR(encode_panel_map(&a.tm_pw[1][v], wBds, n, 0, v == 0));
-                }
+            for (int v = 0; v < 2; ++v) {  // panel tiles, plane [0] and slab [1] views
+                CKR(encode_panel_map(&a.tm_pq[0][v], q, n, (long long)U + 1, v == 0));
+                CKR(encode_panel_map(&a.tm_pq[1][v], qc, n, (long long)U + 1, v == 0));
+                CKR(encode_panel_map(&a.tm_pw[0][v], wAds, n, 0, v == 0));
+                CKR(encode_panel_map(&a.tm_pw[1][v], wBds, n, 0, v == 0));
             }
             CK(cudaMemsetAsync(flags.p, 0, flags.n * sizeof(unsigned), st));
         }
