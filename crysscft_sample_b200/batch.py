@@ -79,8 +79,16 @@ class BatchSCFT:
         wB = np.ascontiguousarray(wB, dtype=np.float64).ravel()
         check(_lib.load().scft_batch_set_fields(self._h, int(i), _lib.dptr(wA), _lib.dptr(wB)))
 
-    def get_fields(self, i: int):
-        out = [np.empty(self.M[i]) for _ in range(4)]
+    def get_fields(self, i: int, out=None):
+        """phiA, phiB, wA, wB of instance i; `out` (four contiguous float64 arrays of the
+        instance's physical grid size, e.g. page-locked ones) receives them instead of new arrays."""
+        if out is None:
+            out = [np.empty(self.M[i]) for _ in range(4)]
+        else:
+            out = list(out)
+            if len(out) != 4 or any(a.dtype != np.float64 or a.size != self.M[i] or not a.flags.c_contiguous
+                                    for a in out):
+                raise ValueError("out must be four contiguous float64 arrays of the instance's grid size")
         check(_lib.load().scft_batch_get_fields(self._h, int(i), *[_lib.dptr(a) for a in out]))
         return dict(zip(("phiA", "phiB", "wA", "wB"), out))
 

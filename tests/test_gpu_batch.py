@@ -36,6 +36,15 @@ def test_batch_matches_single_instance_runs(gpu):
         hs = _single(it, 4)
         assert np.allclose(hb["F"][:, i], hs["F"], rtol=1e-12, atol=0)
         assert np.abs(B.get_fields(i)["phiA"] - hs["phiA"]).max() < 1e-13
+    # caller-provided output arrays receive the same fields
+    for i in range(len(inst)):
+        out = [np.full(B.M[i], np.nan) for _ in range(4)]
+        got = B.get_fields(i, out=out)
+        want = B.get_fields(i)
+        assert all(got[k] is out[j] for j, k in enumerate(("phiA", "phiB", "wA", "wB")))
+        assert all(np.array_equal(got[k], want[k]) for k in want)
+    with pytest.raises(ValueError):
+        B.get_fields(0, out=[np.empty(3)] * 4)
 
 
 def test_batch_instance_matches_reference(gpu):
