@@ -1103,7 +1103,7 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
             }
             fence_async_smem();
             __syncthreads();
-            if (warp == 0 && threadIdx.x == 0) {
+            if (threadIdx.x == 0) {  // the thread that commits and waits on bulk groups
                 tma_store_5d(&a.tm_pq[c][plane ? 0 : 1], QS, 0, 0, 0, p, (int)(slot0 + (long long)dir * k));
                 bulk_commit();
             }
