@@ -47,6 +47,11 @@ SIZES = [
     ("PMMM", (96, 64, 32), 3),
     ("3M", (36, 32, 48), 3),
     ("P1", (128, 32, 16), 2),
+    # alternating kernel with 5, 6 and 7 column panels per tile (40^3 one level, 48^3 even/odd,
+    # 56^3 one level)
+    ("P1", (40, 40, 40), 2),
+    ("PMMM", (96, 96, 96), 2),
+    ("P1", (56, 56, 56), 2),
 ]
 
 
