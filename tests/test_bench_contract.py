@@ -33,3 +33,16 @@ def test_reference_arm_nonzero_rank_exits_quietly():
                           "--steps", "1"], capture_output=True, text=True, timeout=120,
                          env=dict(os.environ, RANK="1", WORLD_SIZE="2"))
     assert out.returncode == 0 and out.stdout.strip() == ""
+
+
+def test_hbm_peak_reads_measured_file_or_falls_back(tmp_path, monkeypatch):
+    sys.path.insert(0, ROOT)
+    import bench
+
+    peak, src = bench.hbm_peak()
+    assert peak > 0 and src in ("measured", "fallback")
+    monkeypatch.setattr(bench, "ROOT", str(tmp_path))
+    assert bench.hbm_peak() == (6650.0, "fallback")
+    (tmp_path / "MEASURED_PEAKS.json").write_text(json.dumps({"hbm_gbs": 6500.5}))
+    assert bench.hbm_peak() == (6500.5, "measured")
+    assert isinstance(bench.cpu_model(), str) and bench.cpu_model()
