@@ -224,6 +224,41 @@ def accuracy_protocol(run, ref_run, start, n_fp32: int, n_polish: int):
                                      np.abs(got["phiB"] - want["phiB"]).max()))}
 
 
+def drop_in_triplets(solver, stream, M: int, n_dev: int = 400, n_host: int = 100):
+    """Triplets/s through the per-triplet boundary the reference's driver calls
+    (CrysPSSolverBase::diffusion, src/crysSCFT_sample.cpp:390): scft_solver_diffusion_device on
+    a resident field (device-timed, back to back), and scft_solver_diffusion on the solver's
+    pinned host iomat (copy in, triplet, copy out, synchronous; wall-timed like the
+    reference's own loop)."""
+    import numpy as np
+    import torch
+
+    rng = np.random.default_rng(5)
+    q = torch.tensor(rng.random(M) + 0.5, dtype=torch.float64, device="cuda")
+    for _ in range(5):
+        solver.diffusion_device(q, stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(n_dev):
+        solver.diffusion_device(q, stream)  # the mean is kept (exp(-k^2 ds) = 1 at k = 0)
+    e1.record(stream)
+    e1.synchronize()
+    dev_ms = e0.elapsed_time(e1)
+    io = solver.get_iomat_for_diffusion()
+    io[:] = rng.random(M) + 0.5
+    for _ in range(3):
+        solver.diffusion()
+    t0 = time.perf_counter()
+    for _ in range(n_host):
+        solver.diffusion()
+    host_s = time.perf_counter() - t0
+    return {"device_triplets_per_s": n_dev / (dev_ms / 1e3),
+            "host_iomat_triplets_per_s": n_host / host_s,
+            "entry_points": "scft_solver_diffusion_device (device-timed), scft_solver_diffusion (host iomat, wall-timed, 2 x M x 8 bytes copied "
+                            "per triplet)"}
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -257,60 +292,66 @@ def run_ours(args):
 
     # ---- device-resident timed region ------------------------------------
     # precision form: K - P iterations with FP32 triplets, then P = K/10 FP64 polish iterations
-    polish = max(1, args.steps // 10) if args.precision == "fp32" else 0
-    if polish:
-        run.set_precision("fp32")
-        run.iterate(max(args.warmup, 3))
-        run.set_precision("fp64")
-        run.iterate(1)  # both launch plans captured before timing
-        run.set_precision("fp32")
-    else:
-        run.iterate(max(args.warmup, 3))
+    polish = max(1, args.steps // 10)
+    run.set_precision("fp32")
+    run.iterate(max(args.warmup, 3))
+    run.set_precision("fp64")
+    run.iterate(max(args.warmup, 3))  # both launch plans captured and warm before timing
     start_fields = run.get_fields()
-    barrier()
-    clocks = ClockSampler(local)
-    clocks.start()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    barrier()
-    ev0.record(stream)
-    if polish:
+
+    def timed(fn):
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        e1.synchronize()
+        barrier()
+        return out, e0.elapsed_time(e1)
+
+    def plain():
+        run.set_fields(start_fields["wA"], start_fields["wB"])
+        run.set_precision("fp64")
+        return run.iterate(args.steps)
+
+    def precision_form_run():
+        run.set_fields(start_fields["wA"], start_fields["wB"])
+        run.set_precision("fp32")
         h1 = run.iterate(args.steps - polish)
         run.set_precision("fp64")
         h2 = run.iterate(polish)
-        hist = {k: np.concatenate([h1[k], h2[k]]) for k in h2}
-    else:
-        hist = run.iterate(args.steps)
-    ev1.record(stream)
-    ev1.synchronize()
-    barrier()
+        return {k: np.concatenate([h1[k], h2[k]]) for k in h2}
+
+    primary = precision_form_run if args.precision == "fp32" else plain
+    secondary = plain if args.precision == "fp32" else precision_form_run
+    clocks = ClockSampler(local)
+    clocks.start()
+    hist, ms = timed(primary)
+    hist2, ms2 = timed(secondary)
     clk = clocks.stop()
-    ms = ev0.elapsed_time(ev1)
-    precision_form = None
-    if polish:
-        # speed: the same K iterations in plain FP64 from the same fields
-        ref_run = scft.DiblockSCFT(solver, WORKLOAD["fA"], WORKLOAD["ds"], WORKLOAD["xN"], WORKLOAD["acc"])
-        ref_run.set_fields(start_fields["wA"], start_fields["wB"])
-        e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e2.record(stream)
-        href = ref_run.iterate(args.steps)
-        e3.record(stream)
-        e3.synchronize()
-        fp64_ms = e2.elapsed_time(e3)
-        dF_timed = abs(hist["F"][-1] - href["F"][-1]) / abs(href["F"][-1])
-        # accuracy on the precision form's protocol: 90 FP32 iterations and 10 FP64 polish
-        # iterations against 100 FP64 iterations, both from the same fields
-        acc = accuracy_protocol(run, ref_run, start_fields, 90, 10)
-        ref_run.close()
-        precision_form = {"fp32_iterations": args.steps - polish, "fp64_polish_iterations": polish,
-                          "protocol": "90 FP32 + 10 FP64 polish iterations vs 100 FP64 iterations, same start",
-                          "dF_over_F": acc["dF_over_F"], "phi_max_abs": acc["phi_max_abs"],
-                          "target": 1e-8, "meets_target": bool(acc["dF_over_F"] <= 1e-8),
-                          "dF_over_F_timed_run": dF_timed,
-                          "timed_run": (f"{args.steps - polish} FP32 + {polish} FP64 iterations vs {args.steps} FP64 "
-                                        "iterations from the same fields (the target is stated on the protocol)"),
-                          "fp64_plain_iterations_per_s": world * args.steps / (fp64_ms / 1e3),
-                          "speedup_vs_fp64_plain": (fp64_ms / ms)}
-        run.set_precision("fp32")
+    fp64_ms, prec_ms = (ms2, ms) if args.precision == "fp32" else (ms, ms2)
+    href, hprec = (hist2, hist) if args.precision == "fp32" else (hist, hist2)
+    dF_timed = abs(hprec["F"][-1] - href["F"][-1]) / abs(href["F"][-1])
+    # accuracy on the precision form's protocol: 90 FP32 iterations and 10 FP64 polish
+    # iterations against 100 FP64 iterations, both from the same fields
+    ref_run = scft.DiblockSCFT(solver, WORKLOAD["fA"], WORKLOAD["ds"], WORKLOAD["xN"], WORKLOAD["acc"])
+    acc = accuracy_protocol(run, ref_run, start_fields, 90, 10)
+    ref_run.close()
+    fp64_ms_all = max_over_ranks(fp64_ms)
+    prec_ms_all = max_over_ranks(prec_ms)
+    precision_form = {"fp32_iterations": args.steps - polish, "fp64_polish_iterations": polish,
+                      "iterations_per_s": world * args.steps / (prec_ms_all / 1e3),
+                      "triplets_per_s": world * args.steps / (prec_ms_all / 1e3) * 2 * U,
+                      "fp64_plain_iterations_per_s": world * args.steps / (fp64_ms_all / 1e3),
+                      "speedup_vs_fp64_plain": fp64_ms_all / prec_ms_all,
+                      "protocol": "90 FP32 + 10 FP64 polish iterations vs 100 FP64 iterations, same start",
+                      "dF_over_F": acc["dF_over_F"], "phi_max_abs": acc["phi_max_abs"],
+                      "target": 1e-8, "meets_target": bool(acc["dF_over_F"] <= 1e-8),
+                      "dF_over_F_timed_run": dF_timed,
+                      "timed_run": (f"{args.steps - polish} FP32 + {polish} FP64 iterations vs {args.steps} FP64 "
+                                    "iterations from the same fields (the target is stated on the protocol)"),
+                      "device_ms": prec_ms_all}
+    run.set_precision(args.precision)
     ms = max_over_ranks(ms)
     value = world * args.steps / (ms / 1e3)
     launches = run.launches_per_iteration()
@@ -318,9 +359,23 @@ def run_ours(args):
         raise RuntimeError("non-finite free energy in the timed region")
 
     # ---- phase timer: the triplet kernels' share (roofline) ---------------
+    other = "fp32" if args.precision == "fp64" else "fp64"
+    run.set_precision(other)
+    phases_other = run.time_phases(10)
+    run.set_precision(args.precision)
     phases = run.time_phases(10)
     chain_s = phases[1] / 1e3  # one launch of the contour kernel = all 2U triplets of an iteration
     b = 8 if args.precision == "fp64" else 4
+    fp32_chain_s = (phases_other if args.precision == "fp64" else phases)[1] / 1e3
+    fp32_bytes = 2 * U * 3 * M * 4
+    precision_form["contour_kernel_fp32"] = {
+        "launch_ms": fp32_chain_s * 1e3, "algorithmic_bytes_per_launch": fp32_bytes,
+        "achieved_gbs": fp32_bytes / fp32_chain_s / 1e9,
+        "phases_ms_per_iteration": dict(zip(("total", "triplets", "q_phi", "fields_energy"),
+                                            phases_other if args.precision == "fp64" else phases))}
+
+    # ---- the drop-in per-triplet boundary (CrysPSSolverBase::diffusion) ----
+    drop_in = drop_in_triplets(solver, stream, M)
     # per triplet: read q(s), read exp(-w ds/2), write q(s+1); K generated on chip, not counted
     alg_bytes_launch = 2 * U * 3 * M * b
     achieved = alg_bytes_launch / chain_s / 1e9
@@ -400,6 +455,7 @@ def run_ours(args):
                        "samples": clk["samples"]},
             "F_last": float(hist["F"][-1]),
             "precision_form": precision_form,
+            "drop_in": drop_in,
         }
     if dist is not None:
         dist.barrier()

@@ -46,6 +46,7 @@ SIGNATURES = {
                                            ctypes.c_double, ctypes.POINTER(_vp)]),
     "scft_diblock_destroy": (ctypes.c_int, [_vp]),
     "scft_diblock_get_contour_counts": (ctypes.c_int, [_vp, _szp, _szp]),
+    "scft_diblock_get_solver": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
     "scft_diblock_set_fields": (ctypes.c_int, [_vp, _dp, _dp]),
     "scft_diblock_get_fields": (ctypes.c_int, [_vp, _dp, _dp, _dp, _dp]),
     "scft_diblock_device_fields": (ctypes.c_int, [_vp] + [ctypes.POINTER(_vp)] * 4),

@@ -55,7 +55,16 @@ class BatchSCFT:
         self.kind = kind.upper()
         self.instances = instances
         self.n = n
-        self.M = [int(np.prod([v // (1 if self.kind == "P1" else 2) for v in it["N"]])) for it in instances]
+        self.M = [self._space_size(i) for i in range(n)]
+
+    def _space_size(self, i: int) -> int:
+        """Physical grid size of instance i, as its solver reports it."""
+        L = _lib.load()
+        d, s, m = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_size_t()
+        check(L.scft_batch_instance(self._h, int(i), ctypes.byref(d)))
+        check(L.scft_diblock_get_solver(d, ctypes.byref(s)))
+        check(L.scft_solver_get_space_size_phy(s, ctypes.byref(m)))
+        return int(m.value)
 
     def close(self):
         if getattr(self, "_h", None):

@@ -30,7 +30,7 @@ namespace crysscft {
 
 static const long double kPi = 3.141592653589793238462643383279502884L;
 
-// g_k = exp(-ds (2 pi k / L)^2): the per-axis factor of K (src/solver_Pmmm.h:380-393,
+// g_k = exp(-ds (2 pi k / L)^2): the per-axis factor of K (src/solver_Pmmm.h:166-179,
 // src/solver_p1.h:149-165, src/solver_3m.h:197-231)
 static long double gauss(long k, long double L, long double ds) {
     long double kk = 2.0L * kPi * (long double)k / L;

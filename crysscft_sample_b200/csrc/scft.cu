@@ -21,6 +21,7 @@
 #include "axis_dmma.cuh"
 #include "axis_kernels.cuh"
 #include "contour_kernel.cuh"
+#include "contour_cluster_f32.cuh"
 #include "contour_kernel_f32.cuh"
 #include "field_kernels.cuh"
 #include "operators.h"
@@ -133,6 +134,11 @@ struct OpsSet {
     std::vector<float> h_packed_f32;
     DevBuf<float> f_packed;
     int eo_f32[3] = {0, 0, 0};
+    // FP32 precision form on clusters (64-point even/odd axes): per axis the fp16 parts
+    // [E_hi | E_lo | O_hi | O_lo] in the tensor cores' K-major operand layout
+    std::vector<uint16_t> h_packed_h16;
+    DevBuf<__half> h16_packed;
+    int h16_axes = 0;  // axes packed (3: the cluster kernel can run)
     // cell-length derivatives dA/dL of the three axis operators (built on first use)
     DevBuf<double> d_dop[3], d_dopT[3];
     bool have_dop = false;
@@ -189,6 +195,53 @@ void pack_operator_f32(const std::vector<long double>& A, int n, OpsSet& s, int 
                 put((size_t)i * ld + j, A[(size_t)i * n + j]);
             }
         }
+}
+
+// fp16 value of v rounded to nearest (ties to even), as its 16-bit pattern; v is finite
+// and below 65504 in magnitude (operator entries and their 2^12-scaled residuals)
+uint16_t half_bits_rn(long double v) {
+    // quantum of the fp16 grid at |v|: 2^(e - 10) for normal values, 2^-24 below 2^-14
+    const long double a = fabsl(v);
+    int e = 0;
+    if (a > 0) frexpl(a, &e);  // a = m 2^e, m in [0.5, 1): the leading bit is 2^(e - 1)
+    const int lead = a > 0 ? e - 1 : -14;
+    const long double quantum = ldexpl(1.0L, (lead < -14 ? -14 : lead) - 10);
+    const long double qv = nearbyintl(v / quantum) * quantum;  // round half to even (default mode)
+    return __half_as_ushort(__float2half_rn((float)qv));          // exact: qv lies on the fp16 grid
+}
+
+// Append one axis operator (64 x 64, centrosymmetric) as the fp16 operator parts of the
+// cluster kernel: E = (A[i][j] + A[i][63-j]) / 2, O = (A[i][j] - A[i][63-j]) / 2 (32 x 32),
+// each split into hi = fp16(x) and lo = fp16((x - hi) 2^12), stored in the canonical K-major
+// layout of a tcgen05 operand (row i = output, k = j: element (i, j) at byte
+// (i / 8) 512 + (j / 8) 128 + (i % 8) 16 + (j % 8) 2).  Returns false (nothing appended)
+// for other operators.
+bool pack_operator_h16(const std::vector<long double>& A, int n, OpsSet& s) {
+    if (n != kClN) return false;
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) {
+            const long double a = A[(size_t)i * n + j], b = A[(size_t)(n - 1 - i) * n + (n - 1 - j)];
+            if (fabsl(a - b) > 1e-17L * (1.0L + fabsl(a))) return false;
+            if (!(fabsl(a) < 8.0L)) return false;  // fp16 range with room for the even/odd sums
+        }
+    const int h = n / 2;
+    const size_t base = s.h_packed_h16.size();
+    s.h_packed_h16.resize(base + (size_t)kClOpAxis, 0);
+    uint16_t* out = s.h_packed_h16.data() + base;
+    auto at = [](int i, int j) { return (size_t)((i / 8) * 256 + (j / 8) * 64 + (i % 8) * 8 + (j % 8)); };
+    for (int i = 0; i < h; ++i)
+        for (int j = 0; j < h; ++j) {
+            const long double a = A[(size_t)i * n + j], b = A[(size_t)i * n + (n - 1 - j)];
+            const long double parts[2] = {(a + b) / 2, (a - b) / 2};
+            for (int m = 0; m < 2; ++m) {
+                const uint16_t hi = half_bits_rn(parts[m]);
+                const long double hv = (long double)__half2float(__ushort_as_half(hi));
+                out[(size_t)(2 * m) * kClOpMat + at(i, j)] = hi;
+                out[(size_t)(2 * m + 1) * kClOpMat + at(i, j)] = half_bits_rn((parts[m] - hv) * 4096.0L);
+            }
+        }
+    ++s.h16_axes;
+    return true;
 }
 
 // Append one axis operator to the packed buffer, in even/odd form when A is
@@ -532,6 +585,7 @@ struct scft_solver_s {
             CKR(upload_operator(A, (int)grid_phy[ax], *s, ax));
             pack_operator(A, (int)grid_phy[ax], *s, ax);
             pack_operator_f32(A, (int)grid_phy[ax], *s, ax);
+            if (nt == 1 && s->h16_axes == ax) pack_operator_h16(A, (int)grid_phy[ax], *s);
             eo2_axes += (kind == SCFT_SOLVER_PMMM && nt == 1 && pack_operator_eo2(A, (int)grid_phy[ax], *s)) ? 1 : 0;
         }
         s->eo2 = eo2_axes == 3;
@@ -546,6 +600,11 @@ struct scft_solver_s {
         CKR(s->f_packed.alloc(s->h_packed_f32.size()));
         CK(cudaMemcpy(s->f_packed.p, s->h_packed_f32.data(), s->h_packed_f32.size() * sizeof(float),
                       cudaMemcpyHostToDevice));
+        if (s->h16_axes == 3) {
+            CKR(s->h16_packed.alloc(s->h_packed_h16.size()));
+            CK(cudaMemcpy(s->h16_packed.p, s->h_packed_h16.data(), s->h_packed_h16.size() * sizeof(uint16_t),
+                          cudaMemcpyHostToDevice));
+        }
         ops = s.get();
         ops_cache[ds_] = std::move(s);
         ++ops_gen;
@@ -763,6 +822,7 @@ struct scft_diblock_s {
     int last_iter_precision = -1;         // precision of the iteration whose contour is stored
     DevBuf<double> stress_buf;            // batched temporaries of scft_diblock_stress
     ContourFnF contour_fn_f32 = nullptr;  // FP32 (3xTF32) contour kernel
+    bool cluster_f32 = false;             // FP32 runs on the cluster kernel (contour_cluster_f32.cuh)
     DevBuf<float> f_xch;                  // FP32 exchange buffers
     DevBuf<unsigned> ctrl;                // [0] barrier arrivals, [1] error bits
     long long spin_limit = 20000000LL;
@@ -789,8 +849,81 @@ struct scft_diblock_s {
     // Decide whether the persistent contour kernel can run this grid (FP64, every
     // axis a multiple of 8 and at most kContourMaxN, shared memory within the limit).
     // FP32 precision form: the 3xTF32 alternating kernel for cubic grids it covers
+    // FP32 on clusters: 64^3 grids whose three axis operators are centrosymmetric (PMMM,
+    // P1), when two 16-CTA clusters with the kernel's shared memory can be resident
+    int setup_cluster_f32() {
+        cluster_f32 = false;
+        const OpsSet* o = solver->ops;
+        if (!o || o->h16_axes != 3 || !o->h16_packed.p || force_form != 0) return SCFT_OK;
+        const size_t* g = solver->grid_phy;
+        if (g[0] != (size_t)kClN || g[1] != (size_t)kClN || g[2] != (size_t)kClN) return SCFT_OK;
+        {
+            const char* e = getenv("CRYSSCFT_FP32_CLUSTER");
+            if (!e || e[0] != '1') return SCFT_OK;
+        }
+        int dev_smem = 0;
+        CK(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, solver->device));
+        if (kClSmem > (size_t)dev_smem) return SCFT_OK;
+        CK(cudaFuncSetAttribute(contour_cluster_kernel_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClSmem));
+        CK(cudaFuncSetAttribute(contour_cluster_kernel_f32, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        cudaLaunchConfig_t cfg{};
+        cudaLaunchAttribute attr[1];
+        cluster_config(cfg, attr, nullptr);
+        int nclusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&nclusters, contour_cluster_kernel_f32, &cfg) != cudaSuccess) {
+            cudaGetLastError();
+            return SCFT_OK;
+        }
+        if (nclusters < 2) return SCFT_OK;
+        if (!ctrl.p) {
+            CKR(ctrl.alloc(2));
+            CK(cudaMemset(ctrl.p, 0, 2 * sizeof(unsigned)));
+        }
+        cluster_f32 = true;
+        persistent = true;
+        alternating = true;
+        return SCFT_OK;
+    }
+
+    void cluster_config(cudaLaunchConfig_t& cfg, cudaLaunchAttribute* attr, cudaStream_t st) const {
+        cfg.gridDim = dim3(2 * kClCtas);
+        cfg.blockDim = dim3(kClThreads);
+        cfg.dynamicSmemBytes = kClSmem;
+        cfg.stream = st;
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = kClCtas;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+    }
+
+    int launch_cluster_f32(cudaStream_t st, float* wAds, float* wBds, float* q, float* qc) {
+        ClusterArgsF a{};
+        a.q[0] = q;
+        a.q[1] = qc;
+        a.wds[0] = wAds;
+        a.wds[1] = wBds;
+        a.ops = solver->ops->h16_packed.p;
+        a.slot0[0] = 0;
+        a.dir[0] = 1;
+        a.slot0[1] = (long long)U;
+        a.dir[1] = -1;
+        a.NsA = (long long)NsA;
+        a.U = (int)U;
+        a.error = reinterpret_cast<int*>(ctrl.p + 1);
+        a.spin_limit = spin_limit;
+        cudaLaunchConfig_t cfg{};
+        cudaLaunchAttribute attr[1];
+        cluster_config(cfg, attr, st);
+        CK(cudaLaunchKernelEx(&cfg, contour_cluster_kernel_f32, a));
+        return SCFT_OK;
+    }
+
     int setup_persistent_f32() {
         persistent = false;
+        CKR(setup_cluster_f32());
+        if (cluster_f32) return SCFT_OK;
         const OpsSet* o = solver->ops;
         if (!o) return SCFT_OK;
         const int nx = (int)solver->grid_phy[0], ny = (int)solver->grid_phy[1], nz = (int)solver->grid_phy[2];
@@ -822,6 +955,7 @@ struct scft_diblock_s {
     }
 
     int launch_contour_f32(cudaStream_t st, float* wAds, float* wBds, float* q, float* qc) {
+        if (cluster_f32) return launch_cluster_f32(st, wAds, wBds, q, qc);
         ContourArgsF a{};
         a.q[0] = q;
         a.q[1] = qc;
@@ -1466,6 +1600,12 @@ int scft_diblock_get_contour_counts(scft_diblock_t d, size_t* NsA, size_t* NsB) 
     return SCFT_OK;
 }
 
+int scft_diblock_get_solver(scft_diblock_t d, scft_solver_t* out) {
+    if (!d || !out) return fail(SCFT_ERR_INVALID_ARG, "null argument");
+    *out = d->solver;
+    return SCFT_OK;
+}
+
 int scft_diblock_set_fields(scft_diblock_t d, const double* wA, const double* wB) {
     if (!d || !wA || !wB) return fail(SCFT_ERR_INVALID_ARG, "null argument");
     CK(cudaSetDevice(d->solver->device));
@@ -1543,8 +1683,11 @@ int scft_diblock_get_fields(scft_diblock_t d, double* phiA, double* phiB, double
 
 int scft_diblock_stress(scft_diblock_t d, double dlnQ_dL[3], double* dF_dxN, double* Q_out) {
     if (!d) return fail(SCFT_ERR_INVALID_ARG, "null handle");
-    if (d->last_iter_precision != SCFT_FP64)
-        return fail(SCFT_ERR_NOT_READY, "the stress needs the stored contour of an FP64 iteration");
+    if (d->last_iter_precision != SCFT_FP64 && d->last_iter_precision != SCFT_FP32)
+        return fail(SCFT_ERR_NOT_READY, "no iteration has run");
+    // the contour of the last iteration: FP64, or FP32 after a precision-form iteration (its
+    // values are promoted; the derivative triplets and the sums stay FP64)
+    const bool f32 = d->last_iter_precision == SCFT_FP32;
     scft_solver_t s = d->solver;
     CK(cudaSetDevice(s->device));
     if (!s->ds_set || !s->ops || s->ds != d->ds) CKR(scft_solver_set_contour_step(s, d->ds));
@@ -1583,13 +1726,20 @@ int scft_diblock_stress(scft_diblock_t d, double dlnQ_dL[3], double* dF_dxN, dou
         for (int blk = 0; blk < 2; ++blk) {
             const long long lo = blk == 0 ? 0 : NsA, hi = blk == 0 ? NsA : U;
             const double* D = blk == 0 ? d->d_wAds.p : d->d_wBds.p;
+            const float* Df = blk == 0 ? d->f_wAds.p : d->f_wBds.p;
             for (long long t0 = lo; t0 < hi; t0 += tc) {
                 const long long nt = std::min(tc, hi - t0);
-                stress_scale_kernel<<<grid_blocks(nt * M, 256), 256, 0, st>>>(X, d->d_q.p, D, t0, nt, M);
+                if (f32)
+                    stress_scale_kernel<float><<<grid_blocks(nt * M, 256), 256, 0, st>>>(X, d->f_q.p, Df, t0, nt, M);
+                else
+                    stress_scale_kernel<double><<<grid_blocks(nt * M, 256), 256, 0, st>>>(X, d->d_q.p, D, t0, nt, M);
                 CK(cudaGetLastError());
                 CKR(s->triplet_batched(X, Y, T1, T2, nt, op, opT, st));
                 const int nb = (int)std::min<long long>(rblocks, (nt * M + kRedThreads - 1) / kRedThreads);
-                stress_dot_kernel<<<nb, kRedThreads, 0, st>>>(d->d_qc.p, D, Y, t0, nt, M, d->partials.p);
+                if (f32)
+                    stress_dot_kernel<float><<<nb, kRedThreads, 0, st>>>(d->f_qc.p, Df, Y, t0, nt, M, d->partials.p);
+                else
+                    stress_dot_kernel<double><<<nb, kRedThreads, 0, st>>>(d->d_qc.p, D, Y, t0, nt, M, d->partials.p);
                 CK(cudaGetLastError());
                 CK(cudaMemcpyAsync(part.data(), d->partials.p, nb * sizeof(double), cudaMemcpyDeviceToHost, st));
                 CK(cudaStreamSynchronize(st));
@@ -2017,18 +2167,33 @@ int scft_batch_autotune(scft_batch_t b, size_t n_trial, size_t* best_nstreams, i
     if (!b || n_trial == 0) return fail(SCFT_ERR_INVALID_ARG, "bad argument");
     CK(cudaSetDevice(b->device));
     const size_t n = b->runs.size();
-    const size_t M0 = b->runs[0]->M;
-    (void)M0;
-    // the trials advance the fields: keep them and put them back afterwards
-    std::vector<std::vector<double>> keepA(n), keepB(n);
+    // The trials advance the fields and change the configuration.  A guard puts the
+    // fields back and destroys the timing events on every exit; on an early (error) exit
+    // it also restores the configuration the batch had before the call.
+    struct Guard {
+        scft_batch_t b;
+        std::vector<std::vector<double>> keepA, keepB;
+        size_t ns0;
+        int form0;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        bool keep_config = false;
+        ~Guard() {
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+            cudaStreamSynchronize(b->main);
+            if (!keep_config) scft_batch_configure(b, ns0, form0);
+            for (size_t i = 0; i < keepA.size(); ++i)
+                if (!keepA[i].empty()) scft_diblock_set_fields(b->runs[i], keepA[i].data(), keepB[i].data());
+        }
+    } g{b, std::vector<std::vector<double>>(n), std::vector<std::vector<double>>(n), b->nstreams, b->form};
     for (size_t i = 0; i < n; ++i) {
-        keepA[i].resize(b->runs[i]->M);
-        keepB[i].resize(b->runs[i]->M);
-        CKR(scft_diblock_get_fields(b->runs[i], nullptr, nullptr, keepA[i].data(), keepB[i].data()));
+        std::vector<double> a(b->runs[i]->M), bb(b->runs[i]->M);
+        CKR(scft_diblock_get_fields(b->runs[i], nullptr, nullptr, a.data(), bb.data()));
+        g.keepA[i] = std::move(a);
+        g.keepB[i] = std::move(bb);
     }
-    cudaEvent_t e0, e1;
-    CK(cudaEventCreate(&e0));
-    CK(cudaEventCreate(&e1));
+    CK(cudaEventCreate(&g.e0));
+    CK(cudaEventCreate(&g.e1));
     double best = 1e300;
     size_t bs = b->nstreams;
     int bf = b->form;
@@ -2039,12 +2204,12 @@ int scft_batch_autotune(scft_batch_t b, size_t n_trial, size_t* best_nstreams, i
             if (ns > n && ns != cand_streams[0]) continue;
             CKR(scft_batch_configure(b, ns, f));
             CKR(b->run(1, nullptr, nullptr));  // capture + warm up
-            CK(cudaEventRecord(e0, b->main));
+            CK(cudaEventRecord(g.e0, b->main));
             CKR(b->run(n_trial, nullptr, nullptr));
-            CK(cudaEventRecord(e1, b->main));
-            CK(cudaEventSynchronize(e1));
+            CK(cudaEventRecord(g.e1, b->main));
+            CK(cudaEventSynchronize(g.e1));
             float ms = 0.f;
-            CK(cudaEventElapsedTime(&ms, e0, e1));
+            CK(cudaEventElapsedTime(&ms, g.e0, g.e1));
             if (ms < best) {
                 best = ms;
                 bs = ns;
@@ -2052,10 +2217,8 @@ int scft_batch_autotune(scft_batch_t b, size_t n_trial, size_t* best_nstreams, i
             }
         }
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     CKR(scft_batch_configure(b, bs, bf));
-    for (size_t i = 0; i < n; ++i) CKR(scft_diblock_set_fields(b->runs[i], keepA[i].data(), keepB[i].data()));
+    g.keep_config = true;  // the guard now only restores the fields and frees the events
     if (best_nstreams) *best_nstreams = bs;
     if (best_form) *best_form = bf;
     if (best_ms) *best_ms = best / (double)n_trial;
@@ -2096,7 +2259,29 @@ static __device__ __align__(256) double g_static_triplet_scratch[2 * SCFT_STATIC
 namespace {
 constexpr int kMaxStaticDevices = 64;
 std::mutex g_static_scratch_mu;
-double* g_static_scratch_dev[kMaxStaticDevices] = {};  // device address per ordinal, set once
+// device address of the array per ordinal, and the context it was looked up in: after a
+// cudaDeviceReset the primary context (and with it the module holding the array) is
+// created anew, so an address saved under the old context is looked up again
+struct StaticScratchAddr {
+    CUcontext ctx = nullptr;
+    double* p = nullptr;
+};
+StaticScratchAddr g_static_scratch_dev[kMaxStaticDevices];
+
+// cuCtxGetCurrent of the driver, resolved once (the library links the runtime only)
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+CtxGetCurrentFn ctx_get_current() {
+    static CtxGetCurrentFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<CtxGetCurrentFn>(p);
+    });
+    return fn;
+}
 }  // namespace
 
 extern "C" int scft_solver_diffusion_device_static_scratch(scft_solver_t s, double* d_io, void* stream) {
@@ -2108,26 +2293,34 @@ extern "C" int scft_solver_diffusion_device_static_scratch(scft_solver_t s, doub
                         std::to_string((size_t)SCFT_STATIC_SCRATCH_MAX_POINTS));
     if (s->device < 0 || s->device >= kMaxStaticDevices)
         return fail(SCFT_ERR_INVALID_ARG, "static-scratch triplet: device ordinal out of range");
+    // rejected before any device work, so a refused call never loads the module on its device
+    if (s->ops->nterms > 1)
+        return fail(SCFT_ERR_UNSUPPORTED,
+                    "static-scratch triplet: a 3m solver with half-cell mirror translations needs a third scratch "
+                    "field; use scft_solver_diffusion_device");
     CK(cudaSetDevice(s->device));
     double* scratch = nullptr;
     {
-        // one-time set-up per device, with that device current: the host-side name of the
-        // array is not a device address, so ask the runtime for the address on this device
+        // set-up once per device (and again after the device's context was replaced), with
+        // that device current: the host-side name of the array is not a device address, so
+        // ask the runtime for the address on this device
+        CUcontext ctx = nullptr;
+        CtxGetCurrentFn get_ctx = ctx_get_current();
+        if (!get_ctx || get_ctx(&ctx) != CUDA_SUCCESS)
+            return fail(SCFT_ERR_CUDA, "static-scratch triplet: cuCtxGetCurrent is not available");
         std::lock_guard<std::mutex> lock(g_static_scratch_mu);
-        if (!g_static_scratch_dev[s->device]) {
+        StaticScratchAddr& a = g_static_scratch_dev[s->device];
+        if (!a.p || a.ctx != ctx) {
             void* p = nullptr;
             cudaError_t e = cudaGetSymbolAddress(&p, g_static_triplet_scratch);
             if (e != cudaSuccess || !p)
                 return fail(SCFT_ERR_CUDA, std::string("cudaGetSymbolAddress(static scratch): ") +
                                                cudaGetErrorString(e));
-            g_static_scratch_dev[s->device] = static_cast<double*>(p);
+            a.p = static_cast<double*>(p);
+            a.ctx = ctx;
         }
-        scratch = g_static_scratch_dev[s->device];
+        scratch = a.p;
     }
-    if (s->ops->nterms > 1)
-        return fail(SCFT_ERR_UNSUPPORTED,
-                    "static-scratch triplet: a 3m solver with half-cell mirror translations needs a third scratch "
-                    "field; use scft_solver_diffusion_device");
     cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
     // the z pass writes every element of t1 before the y pass reads it, and the y pass
     // writes every element of t2 before the x pass reads it: nothing needs clearing

@@ -11,21 +11,24 @@
 
 namespace crysscft {
 
-// X[i][r] = D[r] * q[(t0 + i) M + r] for i < nt
-__global__ void stress_scale_kernel(double* __restrict__ X, const double* __restrict__ q,
-                                    const double* __restrict__ D, long long t0, long long nt, long long M) {
+// X[i][r] = D[r] * q[(t0 + i) M + r] for i < nt.  T: the stored contour's type (FP32 when
+// the last iteration ran the precision form); the derivative triplets run in FP64.
+template <typename T>
+__global__ void stress_scale_kernel(double* __restrict__ X, const T* __restrict__ q,
+                                    const T* __restrict__ D, long long t0, long long nt, long long M) {
     const long long total = nt * M;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
          e += (long long)gridDim.x * blockDim.x) {
         const long long i = e / M, r = e - i * M;
-        X[e] = D[r] * q[(t0 + i) * M + r];
+        X[e] = (double)D[r] * (double)q[(t0 + i) * M + r];
     }
 }
 
 // partials[block] = sum_{i < nt, r < M} qc[(t0 + i + 1) M + r] * D[r] * Y[i M + r]
 // (deterministic: fixed grid, fixed in-block order; the host sums the partials in order)
+template <typename T>
 __global__ void __launch_bounds__(kRedThreads)
-stress_dot_kernel(const double* __restrict__ qc, const double* __restrict__ D, const double* __restrict__ Y,
+stress_dot_kernel(const T* __restrict__ qc, const T* __restrict__ D, const double* __restrict__ Y,
                   long long t0, long long nt, long long M, double* __restrict__ partials) {
     __shared__ double sh[kRedThreads / 32];
     const long long total = nt * M;
@@ -33,7 +36,7 @@ stress_dot_kernel(const double* __restrict__ qc, const double* __restrict__ D, c
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
          e += (long long)gridDim.x * blockDim.x) {
         const long long i = e / M, r = e - i * M;
-        s += qc[(t0 + i + 1) * M + r] * D[r] * Y[e];
+        s += (double)qc[(t0 + i + 1) * M + r] * (double)D[r] * Y[e];
     }
     s = block_sum(s, sh);
     if (threadIdx.x == 0) partials[blockIdx.x] = s;

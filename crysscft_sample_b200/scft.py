@@ -123,8 +123,9 @@ class DiblockSCFT:
         return tuple(p.value for p in ps)
 
     def stress(self):
-        """Backward pass from the last FP64 iteration: d ln Q / d L (3 axes), dF/dchiN, Q.
-        At the saddle point the stress is dF/dL = -dlnQ_dL."""
+        """Backward pass from the stored contour of the last iteration (FP64, or FP32 after a
+        precision-form iteration): d ln Q / d L (3 axes), dF/dchiN, Q.  At the saddle point
+        the stress is dF/dL = -dlnQ_dL."""
         g = np.zeros(3)
         dx, Q = ctypes.c_double(), ctypes.c_double()
         check(_lib.load().scft_diblock_stress(self._h, _lib.dptr(g), ctypes.byref(dx), ctypes.byref(Q)))

@@ -143,13 +143,18 @@ int scft_diblock_create(scft_solver_t solver, double fA, double ds, double xN, d
                         scft_diblock_t* out);
 int scft_diblock_destroy(scft_diblock_t d);
 int scft_diblock_get_contour_counts(scft_diblock_t d, size_t* NsA, size_t* NsB);
+/* The solver the context was created on (the handle stays owned by its creator, or by the
+ * batch for scft_batch_instance contexts); its getters give the grid and space size. */
+int scft_diblock_get_solver(scft_diblock_t d, scft_solver_t* out);
 
 /* Load wA, wB (space_size_phy doubles each, host). */
 int scft_diblock_set_fields(scft_diblock_t d, const double* wA, const double* wB);
 /* Copy phiA, phiB (of the last iteration) and wA, wB (after its update) to host; any may be NULL. */
 int scft_diblock_get_fields(scft_diblock_t d, double* phiA, double* phiB, double* wA, double* wB);
-/* Backward pass of the differentiation form, from the stored contour of the last (FP64)
- * iteration: dlnQ_dL[a] = d ln Q / d L_a at fixed fields, by the adjoint identity
+/* Backward pass of the differentiation form, from the stored contour of the last
+ * iteration (FP64, or the FP32 contour of a precision-form iteration: its slices and
+ * Boltzmann factors are promoted, the derivative triplets and sums run in FP64, so the
+ * result is the precision form's own stress): dlnQ_dL[a] = d ln Q / d L_a at fixed fields, by the adjoint identity
  * dQ/dL_a = (1/M) sum_t < q+[t+1], D_t (dT/dL_a) D_t q[t] > (one term per contour step;
  * T = A_x (x) A_y (x) A_z, so dT/dL_x = (dA_x/dL_x) (x) A_y (x) A_z).  The stress
  * dF/dL_a equals -dlnQ_dL[a] at the SCFT saddle point (there dF/dphi = 0).  For PMMM
@@ -236,9 +241,11 @@ int scft_diblock_time_phases(scft_diblock_t d, size_t n_iter, double out[4]);
  * 2 x SCFT_STATIC_SCRATCH_MAX_POINTS doubles (4 MiB), held by every GPU that loads
  * the library until the process exits.  Solvers with space_size_phy above
  * SCFT_STATIC_SCRATCH_MAX_POINTS are rejected with SCFT_ERR_INVALID_ARG, and 3m
- * solvers whose triplet has several Kronecker terms with SCFT_ERR_UNSUPPORTED.  The first
- * call on each device looks up the array's device address (cudaGetSymbolAddress);
- * make that first call before any stream capture.  All calls on a device share the
+ * solvers whose triplet has several Kronecker terms with SCFT_ERR_UNSUPPORTED (both
+ * before any device work).  The first call on each device looks up the array's device
+ * address (cudaGetSymbolAddress), and so does the first call after that device's context
+ * was replaced (cudaDeviceReset); make that first call before any stream capture.
+ * All calls on a device share the
  * one array, so calls that overlap on the GPU (different streams, or different
  * host threads) race and corrupt each other's results: serialise them. */
 #define SCFT_STATIC_SCRATCH_MAX_POINTS 262144
@@ -268,8 +275,11 @@ int scft_batch_iterate(scft_batch_t b, size_t n_iter, double* F, double* maxinc)
 /* Worker streams and contour-kernel form (0 automatic, 1 alternating layout, 2 two-phase,
  * 3 per-axis kernels). */
 int scft_batch_configure(scft_batch_t b, size_t nstreams, int form);
-/* Time n_trial batch iterations for each candidate configuration, keep the fastest
- * (the fields are restored afterwards). */
+/* Time n_trial batch iterations for each candidate configuration, keep the fastest.
+ * The fields of every instance are restored afterwards (also when a trial fails; then the
+ * configuration the batch had before the call is restored too).  Restoring the fields
+ * goes through scft_batch_set_fields, so it clears each instance's Anderson mixing
+ * history, as scft_diblock_set_fields does. */
 int scft_batch_autotune(scft_batch_t b, size_t n_trial, size_t* best_nstreams, int* best_form, double* best_ms);
 
 /* Measured FP64 throughput of `device` in TFLOP/s: FMA on the CUDA cores and

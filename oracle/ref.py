@@ -29,9 +29,17 @@ _dp = ctypes.POINTER(ctypes.c_double)
 GPU_DRIVER_PATH = os.path.join(_HERE, "_ref", "libref_gpu_driver.so")
 
 
-def build(ref_src: str = "/root/reference/src") -> None:
+def reference_src() -> str:
+    """The reference's src/ directory: $CRYSSCFT_REFERENCE/src, by default a checkout named
+    `reference` beside this repository."""
+    root = os.environ.get("CRYSSCFT_REFERENCE") or os.path.join(os.path.dirname(os.path.dirname(_HERE)), "reference")
+    return os.path.join(root, "src")
+
+
+def build(ref_src: str | None = None) -> None:
     """Compile oracle/_ref/ from the reference sources (only where they exist); the
     reference-driver-over-GPU-adapters library too when the CUDA library is built."""
+    ref_src = ref_src or reference_src()
     if not os.path.isdir(ref_src):
         return
     targets = ["all", "shim"]
