@@ -19,6 +19,7 @@
 
 #include "../../include/crysscft_b200.h"
 #include "axis_dmma.cuh"
+#include "axis_fft.cuh"
 #include "axis_kernels.cuh"
 #include "contour_kernel.cuh"
 #include "contour_cluster_f32.cuh"
@@ -139,6 +140,12 @@ struct OpsSet {
     std::vector<uint16_t> h_packed_h16;
     DevBuf<__half> h16_packed;
     int h16_axes = 0;  // axes packed (3: the cluster kernel can run)
+    // FFT form of the FP64 axis passes (axis_fft.cuh): per axis the transform length (0: the
+    // axis has none), the extension (0 P1, 1 PMMM mirror, 2 3m interleave), the spectrum g
+    // (1/NF included) and the NF twiddles
+    int fft_nf[3] = {0, 0, 0}, fft_ext[3] = {0, 0, 0};
+    DevBuf<double> d_fft_g[3];
+    DevBuf<double2> d_fft_tw[3];
     // cell-length derivatives dA/dL of the three axis operators (built on first use)
     DevBuf<double> d_dop[3], d_dopT[3];
     bool have_dop = false;
@@ -242,6 +249,58 @@ bool pack_operator_h16(const std::vector<long double>& A, int n, OpsSet& s) {
         }
     ++s.h16_axes;
     return true;
+}
+
+// Tables of the FFT axis pass of one axis: the spectrum of the circulant,
+// g_k = exp(-ds (2 pi min(k, NF - k) / L)^2) / NF (the factor of K in src/solver_p1.h:149-165,
+// src/solver_Pmmm.h:166-179, src/solver_3m.h:197-231, with the transforms' normalisation),
+// and the twiddles exp(-2 pi i m / NF), both in long double rounded once.
+int upload_fft_tables(OpsSet& s, int axis, int nf, int ext, long double L, long double ds) {
+    static const long double kPiL = 3.141592653589793238462643383279502884L;
+    std::vector<double> g((size_t)nf);
+    std::vector<double2> tw((size_t)nf);
+    for (int k = 0; k < nf; ++k) {
+        const long double kk = 2.0L * kPiL * (long double)(k < nf - k ? k : nf - k) / L;
+        g[(size_t)k] = (double)(expl(-ds * kk * kk) / (long double)nf);
+        const long double a = -2.0L * kPiL * (long double)k / (long double)nf;
+        tw[(size_t)k] = make_double2((double)cosl(a), (double)sinl(a));
+    }
+    CKR(s.d_fft_g[axis].alloc((size_t)nf));
+    CKR(s.d_fft_tw[axis].alloc((size_t)nf));
+    CK(cudaMemcpy(s.d_fft_g[axis].p, g.data(), g.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(s.d_fft_tw[axis].p, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    s.fft_nf[axis] = nf;
+    s.fft_ext[axis] = ext;
+    return SCFT_OK;
+}
+
+using AxisFftFn = void (*)(const AxisFftPass);
+
+// The FFT pass kernel of an axis of length n with transform length nf and extension ext.
+AxisFftFn axis_fft_kernel_for(int n, int nf, int ext, size_t* smem) {
+#define CRYSSCFT_FFT_CASE(N_, NF_, EXT_)                         \
+    if (n == N_ && nf == NF_ && ext == EXT_) {                   \
+        *smem = FftShape<N_, NF_, EXT_>::SMEM;                   \
+        return axis_fft_kernel<N_, NF_, EXT_>;                   \
+    }
+    CRYSSCFT_FFT_CASE(64, 64, 0)
+    CRYSSCFT_FFT_CASE(128, 128, 0)
+    CRYSSCFT_FFT_CASE(256, 256, 0)
+    CRYSSCFT_FFT_CASE(32, 64, 1)
+    CRYSSCFT_FFT_CASE(64, 128, 1)
+    CRYSSCFT_FFT_CASE(128, 256, 1)
+    CRYSSCFT_FFT_CASE(32, 64, 2)
+    CRYSSCFT_FFT_CASE(64, 128, 2)
+    CRYSSCFT_FFT_CASE(128, 256, 2)
+#undef CRYSSCFT_FFT_CASE
+    return nullptr;
+}
+
+// Which form runs the FP64 axis passes: CRYSSCFT_AXIS_FORM=fft or =dense forces one (for
+// measurements and tests); the default is the dense form.
+int axis_form_override() {
+    const char* e = getenv("CRYSSCFT_AXIS_FORM");
+    return !e ? 0 : (e[0] == 'f' ? 1 : (e[0] == 'd' ? 2 : 0));
 }
 
 // Append one axis operator to the packed buffer, in even/odd form when A is
@@ -561,6 +620,59 @@ struct scft_solver_s {
     }
 
     int nterms() const { return kind == SCFT_SOLVER_3M ? (int)m3terms.size() : 1; }
+    bool m3_no_half_cells() const {
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b)
+                if (m3sym.half[a][b]) return false;
+        return true;
+    }
+    std::vector<const void*> fft_fn_set;  // FFT kernels granted their dynamic shared memory
+
+    // the three passes of a triplet by FFT (axis_fft.cuh); *done = false if an axis has no
+    // FFT form or the dense form is to run
+    int triplet_fft(int nchain, const ChainIO<double> io[2], double* t1[2], double* t2[2], cudaStream_t st,
+                    bool* done) {
+        *done = false;
+        const OpsSet* o = ops;
+        if (o->nterms != 1) return SCFT_OK;
+        if (axis_form_override() != 1) return SCFT_OK;
+        AxisFftFn f[3];
+        size_t sm[3];
+        for (int ax = 0; ax < 3; ++ax) {
+            if (!o->fft_nf[ax]) return SCFT_OK;
+            f[ax] = axis_fft_kernel_for((int)grid_phy[ax], o->fft_nf[ax], o->fft_ext[ax], &sm[ax]);
+            if (!f[ax]) return SCFT_OK;
+        }
+        if (!sms) CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+        const int nx = (int)grid_phy[0], ny = (int)grid_phy[1], nz = (int)grid_phy[2];
+        for (int ax = 2; ax >= 0; --ax) {
+            bool set = false;
+            for (const void* p : fft_fn_set) set |= p == (const void*)f[ax];
+            if (!set) {
+                CK(cudaFuncSetAttribute(f[ax], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm[ax]));
+                fft_fn_set.push_back((const void*)f[ax]);
+            }
+            AxisFftPass p{};
+            for (int c = 0; c < nchain; ++c) {
+                p.in[c] = ax == 2 ? io[c].in : (ax == 1 ? t1[c] : t2[c]);
+                p.out[c] = ax == 2 ? t1[c] : (ax == 1 ? t2[c] : io[c].out);
+                p.pre[c] = ax == 2 ? io[c].pre : nullptr;
+                p.post[c] = ax == 0 ? io[c].post : nullptr;
+            }
+            p.nchain = nchain;
+            p.tw = o->d_fft_tw[ax].p;
+            p.g = o->d_fft_g[ax].p;
+            p.outer = ax == 2 ? (long long)nx * ny : (ax == 1 ? nx : 1);
+            p.inner = ax == 2 ? 1 : (ax == 1 ? nz : (long long)ny * nz);
+            int per_sm = 1;
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f[ax], kFftThreads, sm[ax]));
+            f[ax]<<<sms * (per_sm > 0 ? per_sm : 1), kFftThreads, sm[ax], st>>>(p);
+            CK(cudaGetLastError());
+        }
+        launches += 3;
+        *done = true;
+        return SCFT_OK;
+    }
 
     int build_ops(double ds_) {
         auto s = std::make_unique<OpsSet>();
@@ -586,6 +698,18 @@ struct scft_solver_s {
             pack_operator(A, (int)grid_phy[ax], *s, ax);
             pack_operator_f32(A, (int)grid_phy[ax], *s, ax);
             if (nt == 1 && s->h16_axes == ax) pack_operator_h16(A, (int)grid_phy[ax], *s);
+            {
+                const int n = (int)grid_phy[ax];
+                int nf = 0, ext = 0;
+                const bool m3_plain = kind == SCFT_SOLVER_3M && nt == 1 && m3sym.par[0] == 0 && m3sym.par[1] == 0 &&
+                                      m3sym.par[2] == 0 && m3_no_half_cells();
+                if (kind == SCFT_SOLVER_P1) nf = n;
+                else if (kind == SCFT_SOLVER_PMMM) { nf = 2 * n; ext = 1; }
+                else if (m3_plain) { nf = 2 * n; ext = 2; }
+                size_t fsm = 0;
+                if (nf && axis_fft_kernel_for(n, nf, ext, &fsm))
+                    CKR(upload_fft_tables(*s, ax, nf, ext, (long double)cell[ax], (long double)ds_));
+            }
             eo2_axes += (kind == SCFT_SOLVER_PMMM && nt == 1 && pack_operator_eo2(A, (int)grid_phy[ax], *s)) ? 1 : 0;
         }
         s->eo2 = eo2_axes == 3;
@@ -673,6 +797,9 @@ struct scft_solver_s {
             if ((const void*)io[c].in == (const void*)io[c].out)
                 return fail(SCFT_ERR_INVALID_ARG, "multi-term triplet: input and output alias");
         if constexpr (sizeof(T) == 8) {
+            bool done = false;
+            CKR(triplet_fft(nchain, io, t1, t2, st, &done));
+            if (done) return SCFT_OK;
             // large cubic grids: the three passes on the FP64 tensor cores (axis_dmma.cuh)
             if (nt == 1 && nx == ny && ny == nz && ops->eo[0] == ops->eo[1] && ops->eo[1] == ops->eo[2]) {
                 AxisDmmaFn f[3];
