@@ -237,6 +237,75 @@ def relax_cell(solver, fA, ds, xN, acceptance, wA, wB, L0, n_outer=40, n_inner=2
     return out
 
 
+def converge(run, tol: float, max_iter: int = 2000, chunk: int = 25, history: int = 20, beta: float = 0.5):
+    """Anderson-mixed iterations (history, beta) until the rms residual of an iteration is
+    below tol or max_iter iterations ran; returns (iterations, last residual, last F)."""
+    run.set_mixing("anderson", history, beta)
+    done, res, F = 0, np.inf, np.nan
+    while done < max_iter:
+        h = run.iterate(min(chunk, max_iter - done))
+        r = run.residuals()
+        done += len(r)
+        res, F = float(r[-1]), float(h["F"][-1])
+        if not np.isfinite(res):
+            raise _lib.ScftError(6, "SCFT diverged while converging")
+        if res < tol:
+            break
+    return done, res, F
+
+
+def relax_cubic_cell(solver, fA, ds, xN, acceptance, wA, wB, L0, tol=1e-8, scf_tol=1e-10, max_outer=25,
+                     simple_start=100, history=20, beta=0.5, fp32_tol=None, max_step=0.25):
+    """Variable-cell relaxation of a cubic cell to a stress-free state: at each cell length L
+    the SCFT equations are converged (simple mixing for `simple_start` iterations at the
+    first cell, then Anderson mixing to an rms residual below scf_tol), the stress
+    dF/dL = -sum_a dlnQ/dL_a comes from the backward pass, and L moves by a secant step on
+    dF/dL (the first step a gradient step).  fp32_tol: the precision form, converging each
+    cell with FP32 triplets to fp32_tol first and polishing in FP64 to scf_tol.  Stops at
+    |dF/dL| <= tol.  Returns the history rows (L, F, dF/dL, FP32 iterations, FP64
+    iterations), the final L, F, stress and fields."""
+    run = DiblockSCFT(solver, fA, ds, xN, acceptance)
+    w = (np.asarray(wA, dtype=np.float64).ravel().copy(), np.asarray(wB, dtype=np.float64).ravel().copy())
+    L, prev = float(L0), None
+    hist = []
+    g = F = np.nan
+    try:
+        for outer in range(max_outer):
+            solver.set_cell_para((L, L, L))
+            run.set_fields(*w)
+            n32 = 0
+            if outer == 0 and simple_start:
+                run.set_precision("fp32" if fp32_tol else "fp64")
+                run.set_mixing("simple")
+                run.iterate(simple_start)
+                if fp32_tol:
+                    n32 += simple_start
+            if fp32_tol:
+                run.set_precision("fp32")
+                k, _, _ = converge(run, fp32_tol, history=history, beta=beta)
+                n32 += k
+            run.set_precision("fp64")
+            n64, res, F = converge(run, scf_tol, history=history, beta=beta)
+            g = -float(run.stress()["dlnQ_dL"].sum())
+            f = run.get_fields()
+            w = (f["wA"], f["wB"])
+            hist.append((L, F, g, n32, n64))
+            if abs(g) <= tol:
+                break
+            if prev is None or prev[1] == g:
+                dL = -g * 10.0  # gradient step; d^2F/dL^2 is O(0.1) for these cells
+            else:
+                dL = -g * (L - prev[0]) / (g - prev[1])
+            dL = float(np.clip(dL, -max_step, max_step))
+            prev = (L, g)
+            L += dL
+        out = {"history": hist, "L": L, "F": F, "stress": g}
+        out.update(run.get_fields())
+        return out
+    finally:
+        run.close()
+
+
 def diblock_scft_simple_iterate(Nx, Ny, Nz, fA, ds, xN, Lx, Ly, Lz, acceptance, Nstep, solvername, solver,
                                 init_func, verbose: bool = True):
     """src/crysSCFT_sample.cpp:426-531 on the GPU: init_func(wA, wB) fills numpy arrays of

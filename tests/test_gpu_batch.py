@@ -83,3 +83,30 @@ def test_autotune_restores_fields(gpu):
     B2.seed_fields()
     h2 = B2.iterate(2)
     assert np.allclose(h["F"], h2["F"], rtol=1e-11, atol=0)
+
+
+def test_batching_configuration_200_iterations(gpu):
+    # the configured batch: 64 seeded PMMM instances, reduced grids from {16, 24, 32, 48, 64}^3,
+    # chiN ~ U[14, 30], fA ~ U[0.2, 0.35], L ~ U[3.8, 5.5], BCC or FCC, 200 iterations each
+    # (ds = 0.01), one graph launch per batch iteration after the autotuner's choice; every
+    # instance against its single-instance run, the three smallest against the reference
+    cfg = batch.batch_config(64)
+    B = batch.BatchSCFT("PMMM", cfg, ds=0.01)
+    B.seed_fields()
+    B.autotune(2)
+    hb = B.iterate(200)
+    assert np.all(np.isfinite(hb["F"]))
+    for i, it in enumerate(cfg):
+        hs = _single(it, 200)
+        rel = np.abs(hb["F"][:, i] - hs["F"]) / np.abs(hs["F"])
+        assert rel.max() <= 1e-10, f"instance {i} ({it['N']}): max |dF/F| {rel.max():.3e}"
+    B.close()
+    small = sorted(range(len(cfg)), key=lambda i: (cfg[i]["N"][0], i))[:3]
+    for i in small:
+        it = cfg[i]
+        wA, wB = fields.seed_fields(it["N"], it["L"], it["phase"], seed=it["seed"])
+        want = ref.RefSolver("PMMM", it["N"]).scft_run(it["fA"], 0.01, it["xN"], (it["L"],) * 3, 0.1, 200,
+                                                       fields.to_physical("PMMM", wA),
+                                                       fields.to_physical("PMMM", wB))
+        rel = np.abs(hb["F"][:, i] - want["F"]) / np.abs(want["F"])
+        assert rel.max() <= 1e-10, f"instance {i} ({it['N']}) vs reference: max |dF/F| {rel.max():.3e}"
