@@ -72,6 +72,7 @@ def test_fft_triplet_matches_reference(gpu, kind, N):
     assert np.abs(got - want).max() < 1e-13
     dense = _triplet(kind, N, q, "dense")
     assert np.abs(got - dense).max() < 1e-13
+    assert not np.array_equal(got, dense)  # two different kernels ran (they round differently)
 
 
 def test_fft_propagation_matches_reference(gpu):
@@ -115,4 +116,5 @@ def test_fft_iterations_match_dense(gpu, kind, n):
             G.close()
     rel = np.abs(out["fft"]["F"] - out["dense"]["F"]) / np.abs(out["dense"]["F"])
     assert rel.max() < 1e-12
+    assert not np.array_equal(out["fft"]["phiA"], out["dense"]["phiA"])  # both forms really ran
     assert np.abs(out["fft"]["phiA"] - out["dense"]["phiA"]).max() < 1e-12
