@@ -159,6 +159,7 @@ __global__ void __launch_bounds__(kFftThreads) axis_fft_kernel(const AxisFftPass
     using S = FftShape<N, NF, EXT>;
     constexpr int T = S::T, LINES = S::LINES;
     extern __shared__ __align__(16) unsigned char fft_raw[];
+    __shared__ long long s_base[LINES];  // offset of element 0 of each line of the tile (-1: none)
     double* buf = reinterpret_cast<double*>(fft_raw);
     double2* xch = reinterpret_cast<double2*>(fft_raw);  // aliases the tile between its uses
     double2* stw = reinterpret_cast<double2*>(fft_raw + S::BUF_BYTES);
@@ -173,27 +174,39 @@ __global__ void __launch_bounds__(kFftThreads) axis_fft_kernel(const AxisFftPass
     const long long tiles_per_chain = (lines + LINES - 1) / LINES;
     const long long tiles = tiles_per_chain * p.nchain;
     const long long stride_line = (long long)N * p.inner;
+    const bool contiguous = p.inner == 1;
+    const long long inner = p.inner;
     for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         const int c = (int)(tile / tiles_per_chain);
         const long long L0 = (tile - (long long)c * tiles_per_chain) * LINES;
         const double* in = p.in[c];
         const double* pre = p.pre[c];
-        __syncthreads();  // the previous tile's stores have read the buffer
+        __syncthreads();  // the previous tile's stores have read the buffer and the line offsets
+        // line offsets of this tile: one division per line, not per element
+        for (int l = tid; l < LINES; l += kFftThreads) {
+            const long long L = L0 + l;
+            long long b = -1;
+            if (L < lines) {
+                const long long o = L / inner;
+                b = o * stride_line + (L - o * inner);
+            }
+            s_base[l] = b;
+        }
+        __syncthreads();
         // load the tile (buf[l][j]), coalesced along j for contiguous lines, along l otherwise
         for (int e = tid; e < LINES * N; e += kFftThreads) {
             int l, j;
-            if (p.inner == 1) {
+            if (contiguous) {
                 l = e / N;
                 j = e - l * N;
             } else {
                 j = e / LINES;
                 l = e - j * LINES;
             }
-            const long long L = L0 + l;
+            const long long b = s_base[l];
             double v = 0.0;
-            if (L < lines) {
-                const long long o = L / p.inner, i = L - o * p.inner;
-                const long long idx = o * stride_line + (long long)j * p.inner + i;
+            if (b >= 0) {
+                const long long idx = b + (long long)j * inner;
                 v = in[idx];
                 if (pre) v *= pre[idx];
             }
@@ -247,17 +260,16 @@ __global__ void __launch_bounds__(kFftThreads) axis_fft_kernel(const AxisFftPass
         const double* post = p.post[c];
         for (int e = tid; e < LINES * N; e += kFftThreads) {
             int l, j;
-            if (p.inner == 1) {
+            if (contiguous) {
                 l = e / N;
                 j = e - l * N;
             } else {
                 j = e / LINES;
                 l = e - j * LINES;
             }
-            const long long L = L0 + l;
-            if (L < lines) {
-                const long long o = L / p.inner, i = L - o * p.inner;
-                const long long idx = o * stride_line + (long long)j * p.inner + i;
+            const long long b = s_base[l];
+            if (b >= 0) {
+                const long long idx = b + (long long)j * inner;
                 double v = buf[l * N + j];
                 if (post) v *= post[idx];
                 out[idx] = v;

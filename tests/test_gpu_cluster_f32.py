@@ -56,25 +56,28 @@ def test_cluster_kernel_tracks_fp64(gpu, kind, N):
 
 
 def test_cluster_kernel_contour_has_no_drift(gpu):
-    # the last stored slice of each chain (200 contour steps) against FP64: the mean
-    # relative difference measures a systematic shrink or growth of the propagators
+    # the last stored slice of each chain (200 contour steps) against FP64: the mean relative
+    # difference measures a systematic shrink or growth of the propagators; it must stay at
+    # the level of the 3xTF32 kernel's (whose precision form meets |dF/F| <= 1e-8)
     N = (128, 128, 128)
     G1, r64, _ = _run("PMMM", N, 1, "fp64")
-    G2, r32, _ = _run("PMMM", N, 1, "fp32", cluster=True)
-    NsA, NsB = r64.NsA, r64.NsB
-    U = NsA + NsB
-    out = []
-    for chain, slot in ((0, U), (1, 0)):
-        a = r64.get_contour(chain, slot)
-        b = r32.get_contour(chain, slot)
-        rel = (b - a) / a
-        out.append((float(rel.mean()), float(np.abs(rel).max())))
-    print(f"\ncontour slot 200 relative difference FP32 - FP64: mean {out[0][0]:.3e} / {out[1][0]:.3e}, "
-          f"max {out[0][1]:.3e} / {out[1][1]:.3e}")
-    for mean, mx in out:
-        assert abs(mean) < 2e-5
-        assert mx < 1e-4
-    for r in (r64, r32):
+    G2, rc, _ = _run("PMMM", N, 1, "fp32", cluster=True)
+    G3, rt, _ = _run("PMMM", N, 1, "fp32", cluster=False)
+    U = r64.NsA + r64.NsB
+    stats = {}
+    for name, r in (("cluster", rc), ("3xTF32", rt)):
+        out = []
+        for chain, slot in ((0, U), (1, 0)):
+            a = r64.get_contour(chain, slot)
+            rel = (r.get_contour(chain, slot) - a) / a
+            out.append((float(rel.mean()), float(np.abs(rel).max())))
+        stats[name] = out
+        print(f"\n{name}: contour slot 200 relative difference FP32 - FP64: mean {out[0][0]:.3e} / {out[1][0]:.3e}, "
+              f"max {out[0][1]:.3e} / {out[1][1]:.3e}")
+    for (mc, xc), (mt, xt) in zip(stats["cluster"], stats["3xTF32"]):
+        assert abs(mc) < 1.5 * abs(mt) + 1e-6
+        assert xc < 1e-4
+    for r in (r64, rc, rt):
         r.close()
-    G1.close()
-    G2.close()
+    for g in (G1, G2, G3):
+        g.close()
