@@ -254,51 +254,73 @@ def converge(run, tol: float, max_iter: int = 2000, chunk: int = 25, history: in
     return done, res, F
 
 
-def relax_cubic_cell(solver, fA, ds, xN, acceptance, wA, wB, L0, tol=1e-8, scf_tol=1e-10, max_outer=25,
-                     simple_start=100, history=20, beta=0.5, fp32_tol=None, max_step=0.25):
+def relax_cubic_cell(solver, fA, ds, xN, acceptance, wA, wB, L0, tol=1e-8, scf_tol=1e-10, max_eval=40,
+                     simple_start=100, history=20, beta=0.5, fp32_tol=None, step0=0.1, max_step=0.4):
     """Variable-cell relaxation of a cubic cell to a stress-free state: at each cell length L
     the SCFT equations are converged (simple mixing for `simple_start` iterations at the
-    first cell, then Anderson mixing to an rms residual below scf_tol), the stress
-    dF/dL = -sum_a dlnQ/dL_a comes from the backward pass, and L moves by a secant step on
-    dF/dL (the first step a gradient step).  fp32_tol: the precision form, converging each
-    cell with FP32 triplets to fp32_tol first and polishing in FP64 to scf_tol.  Stops at
-    |dF/dL| <= tol.  Returns the history rows (L, F, dF/dL, FP32 iterations, FP64
-    iterations), the final L, F, stress and fields."""
+    first cell, then Anderson mixing to an rms residual below scf_tol) and the stress
+    dF/dL = -sum_a dlnQ/dL_a comes from the backward pass.  L first moves downhill (against
+    the sign of dF/dL) with doubling steps until dF/dL changes sign, then the bracketed root
+    is refined by regula falsi (Illinois): a minimum of F(L), not just any zero of the stress.
+    fp32_tol: the precision form, converging each cell with FP32 triplets to fp32_tol first
+    and polishing in FP64 to scf_tol.  Stops at |dF/dL| <= tol.  Returns the history rows
+    (L, F, dF/dL, FP32 iterations, FP64 iterations), the final L, F, stress and fields."""
     run = DiblockSCFT(solver, fA, ds, xN, acceptance)
-    w = (np.asarray(wA, dtype=np.float64).ravel().copy(), np.asarray(wB, dtype=np.float64).ravel().copy())
-    L, prev = float(L0), None
+    state = {"w": (np.asarray(wA, dtype=np.float64).ravel().copy(),
+                   np.asarray(wB, dtype=np.float64).ravel().copy()), "first": True}
     hist = []
-    g = F = np.nan
+
+    def evaluate(L):
+        solver.set_cell_para((L, L, L))
+        run.set_fields(*state["w"])
+        n32 = 0
+        if state["first"] and simple_start:
+            run.set_precision("fp32" if fp32_tol else "fp64")
+            run.set_mixing("simple")
+            run.iterate(simple_start)
+            n32 += simple_start if fp32_tol else 0
+        state["first"] = False
+        if fp32_tol:
+            run.set_precision("fp32")
+            n32 += converge(run, fp32_tol, history=history, beta=beta)[0]
+        run.set_precision("fp64")
+        n64, _, F = converge(run, scf_tol, history=history, beta=beta)
+        g = -float(run.stress()["dlnQ_dL"].sum())
+        f = run.get_fields()
+        state["w"] = (f["wA"], f["wB"])
+        hist.append((L, F, g, n32, n64))
+        return g, F
+
     try:
-        for outer in range(max_outer):
-            solver.set_cell_para((L, L, L))
-            run.set_fields(*w)
-            n32 = 0
-            if outer == 0 and simple_start:
-                run.set_precision("fp32" if fp32_tol else "fp64")
-                run.set_mixing("simple")
-                run.iterate(simple_start)
-                if fp32_tol:
-                    n32 += simple_start
-            if fp32_tol:
-                run.set_precision("fp32")
-                k, _, _ = converge(run, fp32_tol, history=history, beta=beta)
-                n32 += k
-            run.set_precision("fp64")
-            n64, res, F = converge(run, scf_tol, history=history, beta=beta)
-            g = -float(run.stress()["dlnQ_dL"].sum())
-            f = run.get_fields()
-            w = (f["wA"], f["wB"])
-            hist.append((L, F, g, n32, n64))
-            if abs(g) <= tol:
+        L, (g, F) = float(L0), evaluate(float(L0))
+        lo = hi = None
+        step = step0
+        # bracket: walk downhill until the stress changes sign
+        while abs(g) > tol and lo is None and len(hist) < max_eval:
+            Ln = L - np.sign(g) * step
+            gn, Fn = evaluate(Ln)
+            if np.sign(gn) != np.sign(g) or abs(gn) <= tol:
+                lo, hi = ((L, g), (Ln, gn)) if L < Ln else ((Ln, gn), (L, g))
+                L, g, F = Ln, gn, Fn
                 break
-            if prev is None or prev[1] == g:
-                dL = -g * 10.0  # gradient step; d^2F/dL^2 is O(0.1) for these cells
+            L, g, F = Ln, gn, Fn
+            step = min(2 * step, max_step)
+        # refine: regula falsi with the Illinois modification on [lo, hi] (g(lo) < 0 < g(hi))
+        side = 0
+        while abs(g) > tol and lo is not None and len(hist) < max_eval:
+            (La, ga), (Lb, gb) = lo, hi
+            L = (La * gb - Lb * ga) / (gb - ga)
+            g, F = evaluate(L)
+            if g < 0:
+                lo = (L, g)
+                if side == -1:
+                    hi = (hi[0], hi[1] / 2)
+                side = -1
             else:
-                dL = -g * (L - prev[0]) / (g - prev[1])
-            dL = float(np.clip(dL, -max_step, max_step))
-            prev = (L, g)
-            L += dL
+                hi = (L, g)
+                if side == 1:
+                    lo = (lo[0], lo[1] / 2)
+                side = 1
         out = {"history": hist, "L": L, "F": F, "stress": g}
         out.update(run.get_fields())
         return out
