@@ -1,4 +1,4 @@
-// Axis passes by fast Fourier transform (the "butterfly" form of the FP64 triplets).
+// Axis passes by fast Fourier transform (the "butterfly" form of the triplets, FP64 and FP32).
 //
 // Every per-axis operator of the three solvers is a real circulant with an even
 // spectrum g, applied to an extension of the line and restricted back:
@@ -25,18 +25,25 @@ namespace crysscft {
 
 constexpr int kFftThreads = 256;
 
+// complex type of a real type
+template <typename T> struct CplxOf;
+template <> struct CplxOf<double> { using type = double2; };
+template <> struct CplxOf<float> { using type = float2; };
+
+template <typename T>
 struct AxisFftPass {
-    const double* in[2];
-    double* out[2];
-    const double* pre[2];    // input *= pre (nullptr: none)
-    const double* post[2];   // output *= post (nullptr: none)
-    const double2* tw;       // NF twiddles exp(-2 pi i m / NF)
-    const double* g;         // NF spectrum values, 1/NF included
+    using C = typename CplxOf<T>::type;
+    const T* in[2];
+    T* out[2];
+    const T* pre[2];         // input *= pre (nullptr: none)
+    const T* post[2];        // output *= post (nullptr: none)
+    const C* tw;             // NF twiddles exp(-2 pi i m / NF)
+    const T* g;              // NF spectrum values, 1/NF included
     long long outer, inner;  // lines (o, i), element j of line (o, i) at o n inner + j inner + i
     int nchain;
 };
 
-template <int N, int NF, int EXT>
+template <int N, int NF, int EXT, typename R = double>
 struct FftShape {
     static_assert(NF == 64 || NF == 128 || NF == 256, "transform lengths 64, 128, 256");
     static_assert((EXT == 0 && NF == N) || (EXT != 0 && NF == 2 * N), "P1: NF = n; PMMM, 3m: NF = 2n");
@@ -44,10 +51,10 @@ struct FftShape {
     static constexpr int PAIRS = kFftThreads / T;
     static constexpr int LINES = 2 * PAIRS;
     static constexpr int XROW = T + 1;              // exchange row (padded against bank conflicts)
-    static constexpr size_t TILE_BYTES = (size_t)LINES * N * sizeof(double);
-    static constexpr size_t XCH_BYTES = (size_t)PAIRS * 16 * XROW * sizeof(double2);
+    static constexpr size_t TILE_BYTES = (size_t)LINES * N * sizeof(R);
+    static constexpr size_t XCH_BYTES = (size_t)PAIRS * 16 * XROW * 2 * sizeof(R);
     static constexpr size_t BUF_BYTES = TILE_BYTES > XCH_BYTES ? TILE_BYTES : XCH_BYTES;
-    static constexpr size_t SMEM = BUF_BYTES + (size_t)NF * (sizeof(double2) + sizeof(double));
+    static constexpr size_t SMEM = BUF_BYTES + (size_t)NF * 3 * sizeof(R);
 };
 
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
@@ -56,10 +63,20 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
     return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
 }
 __device__ __forceinline__ double2 mul_minus_i(double2 a) { return make_double2(a.y, -a.x); }
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ float2 mul_minus_i(float2 a) { return make_float2(a.y, -a.x); }
+template <typename C> __device__ __forceinline__ C cmake(double x, double y);
+template <> __device__ __forceinline__ double2 cmake<double2>(double x, double y) { return make_double2(x, y); }
+template <> __device__ __forceinline__ float2 cmake<float2>(double x, double y) { return make_float2((float)x, (float)y); }
 
 // in-place 4-point DFT (W4 = -i)
-__device__ __forceinline__ void dft4(double2& a, double2& b, double2& c, double2& d) {
-    const double2 t0 = cadd(a, c), t1 = csub(a, c), t2 = cadd(b, d), t3 = mul_minus_i(csub(b, d));
+template <typename C>
+__device__ __forceinline__ void dft4(C& a, C& b, C& c, C& d) {
+    const C t0 = cadd(a, c), t1 = csub(a, c), t2 = cadd(b, d), t3 = mul_minus_i(csub(b, d));
     a = cadd(t0, t2);
     c = csub(t0, t2);
     b = cadd(t1, t3);
@@ -67,22 +84,24 @@ __device__ __forceinline__ void dft4(double2& a, double2& b, double2& c, double2
 }
 
 // W16^j = exp(-2 pi i j / 16) for the products m2 k1 of a radix-4 x 4 16-point DFT
-__device__ __forceinline__ double2 w16(int j) {
+template <typename C>
+__device__ __forceinline__ C w16(int j) {
     constexpr double c1 = 0.92387953251128675613, s1 = 0.38268343236508977173, h = 0.70710678118654752440;
     switch (j) {
-        case 0: return make_double2(1.0, 0.0);
-        case 1: return make_double2(c1, -s1);
-        case 2: return make_double2(h, -h);
-        case 3: return make_double2(s1, -c1);
-        case 4: return make_double2(0.0, -1.0);
-        case 6: return make_double2(-h, -h);
-        default: return make_double2(-c1, s1);  // j = 9
+        case 0: return cmake<C>(1.0, 0.0);
+        case 1: return cmake<C>(c1, -s1);
+        case 2: return cmake<C>(h, -h);
+        case 3: return cmake<C>(s1, -c1);
+        case 4: return cmake<C>(0.0, -1.0);
+        case 6: return cmake<C>(-h, -h);
+        default: return cmake<C>(-c1, s1);  // j = 9
     }
 }
 
 // out[k] = sum_m x[m] W16^(m k), k = k1 + 4 k2, m = 4 m1 + m2
-__device__ __forceinline__ void dft16(const double2 (&x)[16], double2 (&out)[16]) {
-    double2 y[16];
+template <typename C>
+__device__ __forceinline__ void dft16(const C (&x)[16], C (&out)[16]) {
+    C y[16];
 #pragma unroll
     for (int i = 0; i < 16; ++i) y[i] = x[i];
 #pragma unroll
@@ -90,7 +109,7 @@ __device__ __forceinline__ void dft16(const double2 (&x)[16], double2 (&out)[16]
 #pragma unroll
     for (int m2 = 1; m2 < 4; ++m2)
 #pragma unroll
-        for (int k1 = 1; k1 < 4; ++k1) y[4 * k1 + m2] = cmul(y[4 * k1 + m2], w16(m2 * k1));
+        for (int k1 = 1; k1 < 4; ++k1) y[4 * k1 + m2] = cmul(y[4 * k1 + m2], w16<C>(m2 * k1));
 #pragma unroll
     for (int k1 = 0; k1 < 4; ++k1) dft4(y[4 * k1], y[4 * k1 + 1], y[4 * k1 + 2], y[4 * k1 + 3]);  // -> y[4 k1 + k2]
 #pragma unroll
@@ -100,29 +119,29 @@ __device__ __forceinline__ void dft16(const double2 (&x)[16], double2 (&out)[16]
 }
 
 // R-point DFT (R = 4, 8, 16) of x[0..R-1] in place
-template <int R>
-__device__ __forceinline__ void dft_small(double2* x) {
+template <int R, typename C>
+__device__ __forceinline__ void dft_small(C* x) {
     if constexpr (R == 4) {
         dft4(x[0], x[1], x[2], x[3]);
     } else if constexpr (R == 8) {
         // m = 2 m1 + m2: two 4-point DFTs, W8^k1 on the odd one, radix-2 combine
-        double2 e[4] = {x[0], x[2], x[4], x[6]}, o[4] = {x[1], x[3], x[5], x[7]};
+        C e[4] = {x[0], x[2], x[4], x[6]}, o[4] = {x[1], x[3], x[5], x[7]};
         dft4(e[0], e[1], e[2], e[3]);
         dft4(o[0], o[1], o[2], o[3]);
         constexpr double h = 0.70710678118654752440;
         x[0] = cadd(e[0], o[0]);
         x[4] = csub(e[0], o[0]);
-        const double2 t1 = cmul(o[1], make_double2(h, -h));
+        const C t1 = cmul(o[1], cmake<C>(h, -h));
         x[1] = cadd(e[1], t1);
         x[5] = csub(e[1], t1);
-        const double2 t2 = mul_minus_i(o[2]);
+        const C t2 = mul_minus_i(o[2]);
         x[2] = cadd(e[2], t2);
         x[6] = csub(e[2], t2);
-        const double2 t3 = cmul(o[3], make_double2(-h, -h));
+        const C t3 = cmul(o[3], cmake<C>(-h, -h));
         x[3] = cadd(e[3], t3);
         x[7] = csub(e[3], t3);
     } else {
-        double2 in[16], out[16];
+        C in[16], out[16];
 #pragma unroll
         for (int i = 0; i < 16; ++i) in[i] = x[i];
         dft16(in, out);
@@ -133,10 +152,10 @@ __device__ __forceinline__ void dft_small(double2* x) {
 
 // NF-point forward FFT of one line pair, z[m] = x[T m + t] in, X[T m + t] out.
 // xch: this pair's exchange rows (16 x XROW), tw: the NF twiddles (shared memory).
-template <int NF>
-__device__ __forceinline__ void fft_pair(double2 (&z)[16], double2* xch, const double2* tw, int t) {
+template <int NF, typename Cx>
+__device__ __forceinline__ void fft_pair(Cx (&z)[16], Cx* xch, const Cx* tw, int t) {
     constexpr int T = NF / 16, XROW = T + 1, C = 16 / T;
-    double2 y[16];
+    Cx y[16];
     dft16(z, y);  // y[k1] = sum_{n1} x[T n1 + t] W16^(n1 k1)
 #pragma unroll
     for (int k1 = 0; k1 < 16; ++k1) xch[k1 * XROW + t] = k1 && t ? cmul(y[k1], tw[t * k1]) : y[k1];
@@ -144,7 +163,7 @@ __device__ __forceinline__ void fft_pair(double2 (&z)[16], double2* xch, const d
 #pragma unroll
     for (int c = 0; c < C; ++c) {
         const int k1 = t + T * c;
-        double2 col[T];
+        Cx col[T];
 #pragma unroll
         for (int n2 = 0; n2 < T; ++n2) col[n2] = xch[k1 * XROW + n2];
         dft_small<T>(col);  // col[k2] = X[k1 + 16 k2]
@@ -154,16 +173,17 @@ __device__ __forceinline__ void fft_pair(double2 (&z)[16], double2* xch, const d
     __syncthreads();  // the exchange rows may be written again
 }
 
-template <int N, int NF, int EXT>
-__global__ void __launch_bounds__(kFftThreads) axis_fft_kernel(const AxisFftPass p) {
-    using S = FftShape<N, NF, EXT>;
+template <int N, int NF, int EXT, typename R = double>
+__global__ void __launch_bounds__(kFftThreads) axis_fft_kernel(const AxisFftPass<R> p) {
+    using S = FftShape<N, NF, EXT, R>;
+    using Cx = typename CplxOf<R>::type;
     constexpr int T = S::T, LINES = S::LINES;
     extern __shared__ __align__(16) unsigned char fft_raw[];
     __shared__ long long s_base[LINES];  // offset of element 0 of each line of the tile (-1: none)
-    double* buf = reinterpret_cast<double*>(fft_raw);
-    double2* xch = reinterpret_cast<double2*>(fft_raw);  // aliases the tile between its uses
-    double2* stw = reinterpret_cast<double2*>(fft_raw + S::BUF_BYTES);
-    double* sg = reinterpret_cast<double*>(stw + NF);
+    R* buf = reinterpret_cast<R*>(fft_raw);
+    Cx* xch = reinterpret_cast<Cx*>(fft_raw);  // aliases the tile between its uses
+    Cx* stw = reinterpret_cast<Cx*>(fft_raw + S::BUF_BYTES);
+    R* sg = reinterpret_cast<R*>(stw + NF);
     const int tid = threadIdx.x;
     for (int e = tid; e < NF; e += kFftThreads) {
         stw[e] = p.tw[e];
@@ -179,8 +199,8 @@ __global__ void __launch_bounds__(kFftThreads) axis_fft_kernel(const AxisFftPass
     for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         const int c = (int)(tile / tiles_per_chain);
         const long long L0 = (tile - (long long)c * tiles_per_chain) * LINES;
-        const double* in = p.in[c];
-        const double* pre = p.pre[c];
+        const R* in = p.in[c];
+        const R* pre = p.pre[c];
         __syncthreads();  // the previous tile's stores have read the buffer and the line offsets
         // line offsets of this tile: one division per line, not per element
         for (int l = tid; l < LINES; l += kFftThreads) {
@@ -204,7 +224,7 @@ __global__ void __launch_bounds__(kFftThreads) axis_fft_kernel(const AxisFftPass
                 l = e - j * LINES;
             }
             const long long b = s_base[l];
-            double v = 0.0;
+            R v = R(0);
             if (b >= 0) {
                 const long long idx = b + (long long)j * inner;
                 v = in[idx];
@@ -213,9 +233,9 @@ __global__ void __launch_bounds__(kFftThreads) axis_fft_kernel(const AxisFftPass
             buf[l * N + j] = v;
         }
         __syncthreads();
-        double2 z[16];
-        const double* l1 = buf + (2 * pair) * N;
-        const double* l2 = l1 + N;
+        Cx z[16];
+        const R* l1 = buf + (2 * pair) * N;
+        const R* l2 = l1 + N;
 #pragma unroll
         for (int m = 0; m < 16; ++m) {
             const int k = T * m + t;
@@ -223,20 +243,22 @@ __global__ void __launch_bounds__(kFftThreads) axis_fft_kernel(const AxisFftPass
             if constexpr (EXT == 0) e = k;
             else if constexpr (EXT == 1) e = k < N ? k : 2 * N - 1 - k;
             else e = (k & 1) ? N - 1 - (k >> 1) : (k >> 1);
-            z[m] = make_double2(l1[e], l2[e]);
+            z[m].x = l1[e];
+            z[m].y = l2[e];
         }
         __syncthreads();  // the tile is read: its memory becomes the exchange rows
-        double2* my = xch + (size_t)pair * 16 * S::XROW;
+        Cx* my = xch + (size_t)pair * 16 * S::XROW;
         fft_pair<NF>(z, my, stw, t);
 #pragma unroll
         for (int m = 0; m < 16; ++m) {
-            const double gk = sg[T * m + t];
-            z[m] = make_double2(z[m].x * gk, -z[m].y * gk);
+            const R gk = sg[T * m + t];
+            z[m].x = z[m].x * gk;
+            z[m].y = -z[m].y * gk;
         }
         fft_pair<NF>(z, my, stw, t);
         // results: A x1 = Re, A x2 = -Im, at the kept points of the extension
-        double* o1 = buf + (2 * pair) * N;
-        double* o2 = o1 + N;
+        R* o1 = buf + (2 * pair) * N;
+        R* o2 = o1 + N;
 #pragma unroll
         for (int m = 0; m < 16; ++m) {
             const int k = T * m + t;
@@ -256,8 +278,8 @@ __global__ void __launch_bounds__(kFftThreads) axis_fft_kernel(const AxisFftPass
             }
         }
         __syncthreads();
-        double* out = p.out[c];
-        const double* post = p.post[c];
+        R* out = p.out[c];
+        const R* post = p.post[c];
         for (int e = tid; e < LINES * N; e += kFftThreads) {
             int l, j;
             if (contiguous) {
@@ -270,7 +292,7 @@ __global__ void __launch_bounds__(kFftThreads) axis_fft_kernel(const AxisFftPass
             const long long b = s_base[l];
             if (b >= 0) {
                 const long long idx = b + (long long)j * inner;
-                double v = buf[l * N + j];
+                R v = buf[l * N + j];
                 if (post) v *= post[idx];
                 out[idx] = v;
             }

@@ -146,6 +146,8 @@ struct OpsSet {
     int fft_nf[3] = {0, 0, 0}, fft_ext[3] = {0, 0, 0};
     DevBuf<double> d_fft_g[3];
     DevBuf<double2> d_fft_tw[3];
+    DevBuf<float> f_fft_g[3];   // the same tables rounded to FP32 (precision form)
+    DevBuf<float2> f_fft_tw[3];
     // cell-length derivatives dA/dL of the three axis operators (built on first use)
     DevBuf<double> d_dop[3], d_dopT[3];
     bool have_dop = false;
@@ -269,19 +271,31 @@ int upload_fft_tables(OpsSet& s, int axis, int nf, int ext, long double L, long 
     CKR(s.d_fft_tw[axis].alloc((size_t)nf));
     CK(cudaMemcpy(s.d_fft_g[axis].p, g.data(), g.size() * sizeof(double), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(s.d_fft_tw[axis].p, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    std::vector<float> gf((size_t)nf);
+    std::vector<float2> twf((size_t)nf);
+    for (int k = 0; k < nf; ++k) {
+        gf[(size_t)k] = (float)g[(size_t)k];
+        twf[(size_t)k] = make_float2((float)tw[(size_t)k].x, (float)tw[(size_t)k].y);
+    }
+    CKR(s.f_fft_g[axis].alloc((size_t)nf));
+    CKR(s.f_fft_tw[axis].alloc((size_t)nf));
+    CK(cudaMemcpy(s.f_fft_g[axis].p, gf.data(), gf.size() * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(s.f_fft_tw[axis].p, twf.data(), twf.size() * sizeof(float2), cudaMemcpyHostToDevice));
     s.fft_nf[axis] = nf;
     s.fft_ext[axis] = ext;
     return SCFT_OK;
 }
 
-using AxisFftFn = void (*)(const AxisFftPass);
+template <typename R>
+using AxisFftFn = void (*)(const AxisFftPass<R>);
 
 // The FFT pass kernel of an axis of length n with transform length nf and extension ext.
-AxisFftFn axis_fft_kernel_for(int n, int nf, int ext, size_t* smem) {
+template <typename R>
+AxisFftFn<R> axis_fft_kernel_for(int n, int nf, int ext, size_t* smem) {
 #define CRYSSCFT_FFT_CASE(N_, NF_, EXT_)                         \
     if (n == N_ && nf == NF_ && ext == EXT_) {                   \
-        *smem = FftShape<N_, NF_, EXT_>::SMEM;                   \
-        return axis_fft_kernel<N_, NF_, EXT_>;                   \
+        *smem = FftShape<N_, NF_, EXT_, R>::SMEM;                \
+        return axis_fft_kernel<N_, NF_, EXT_, R>;                \
     }
     CRYSSCFT_FFT_CASE(64, 64, 0)
     CRYSSCFT_FFT_CASE(128, 128, 0)
@@ -630,17 +644,17 @@ struct scft_solver_s {
 
     // the three passes of a triplet by FFT (axis_fft.cuh); *done = false if an axis has no
     // FFT form or the dense form is to run
-    int triplet_fft(int nchain, const ChainIO<double> io[2], double* t1[2], double* t2[2], cudaStream_t st,
-                    bool* done) {
+    template <typename T>
+    int triplet_fft(int nchain, const ChainIO<T> io[2], T* t1[2], T* t2[2], cudaStream_t st, bool* done) {
         *done = false;
         const OpsSet* o = ops;
         if (o->nterms != 1) return SCFT_OK;
         if (axis_form_override() != 1) return SCFT_OK;
-        AxisFftFn f[3];
+        AxisFftFn<T> f[3];
         size_t sm[3];
         for (int ax = 0; ax < 3; ++ax) {
             if (!o->fft_nf[ax]) return SCFT_OK;
-            f[ax] = axis_fft_kernel_for((int)grid_phy[ax], o->fft_nf[ax], o->fft_ext[ax], &sm[ax]);
+            f[ax] = axis_fft_kernel_for<T>((int)grid_phy[ax], o->fft_nf[ax], o->fft_ext[ax], &sm[ax]);
             if (!f[ax]) return SCFT_OK;
         }
         if (!sms) CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
@@ -652,7 +666,7 @@ struct scft_solver_s {
                 CK(cudaFuncSetAttribute(f[ax], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm[ax]));
                 fft_fn_set.push_back((const void*)f[ax]);
             }
-            AxisFftPass p{};
+            AxisFftPass<T> p{};
             for (int c = 0; c < nchain; ++c) {
                 p.in[c] = ax == 2 ? io[c].in : (ax == 1 ? t1[c] : t2[c]);
                 p.out[c] = ax == 2 ? t1[c] : (ax == 1 ? t2[c] : io[c].out);
@@ -660,8 +674,13 @@ struct scft_solver_s {
                 p.post[c] = ax == 0 ? io[c].post : nullptr;
             }
             p.nchain = nchain;
-            p.tw = o->d_fft_tw[ax].p;
-            p.g = o->d_fft_g[ax].p;
+            if constexpr (sizeof(T) == 8) {
+                p.tw = o->d_fft_tw[ax].p;
+                p.g = o->d_fft_g[ax].p;
+            } else {
+                p.tw = o->f_fft_tw[ax].p;
+                p.g = o->f_fft_g[ax].p;
+            }
             p.outer = ax == 2 ? (long long)nx * ny : (ax == 1 ? nx : 1);
             p.inner = ax == 2 ? 1 : (ax == 1 ? nz : (long long)ny * nz);
             int per_sm = 1;
@@ -707,7 +726,7 @@ struct scft_solver_s {
                 else if (kind == SCFT_SOLVER_PMMM) { nf = 2 * n; ext = 1; }
                 else if (m3_plain) { nf = 2 * n; ext = 2; }
                 size_t fsm = 0;
-                if (nf && axis_fft_kernel_for(n, nf, ext, &fsm))
+                if (nf && axis_fft_kernel_for<double>(n, nf, ext, &fsm))
                     CKR(upload_fft_tables(*s, ax, nf, ext, (long double)cell[ax], (long double)ds_));
             }
             eo2_axes += (kind == SCFT_SOLVER_PMMM && nt == 1 && pack_operator_eo2(A, (int)grid_phy[ax], *s)) ? 1 : 0;
@@ -796,10 +815,12 @@ struct scft_solver_s {
         for (int c = 0; c < nchain && nt > 1; ++c)
             if ((const void*)io[c].in == (const void*)io[c].out)
                 return fail(SCFT_ERR_INVALID_ARG, "multi-term triplet: input and output alias");
-        if constexpr (sizeof(T) == 8) {
+        {
             bool done = false;
-            CKR(triplet_fft(nchain, io, t1, t2, st, &done));
+            CKR(triplet_fft<T>(nchain, io, t1, t2, st, &done));
             if (done) return SCFT_OK;
+        }
+        if constexpr (sizeof(T) == 8) {
             // large cubic grids: the three passes on the FP64 tensor cores (axis_dmma.cuh)
             if (nt == 1 && nx == ny && ny == nz && ops->eo[0] == ops->eo[1] && ops->eo[1] == ops->eo[2]) {
                 AxisDmmaFn f[3];

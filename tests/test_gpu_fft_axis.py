@@ -118,3 +118,30 @@ def test_fft_iterations_match_dense(gpu, kind, n):
     assert rel.max() < 1e-12
     assert not np.array_equal(out["fft"]["phiA"], out["dense"]["phiA"])  # both forms really ran
     assert np.abs(out["fft"]["phiA"] - out["dense"]["phiA"]).max() < 1e-12
+
+
+@pytest.mark.parametrize("kind,n", [("PMMM", 256), ("P1", 128)])
+def test_fp32_fft_iterations_track_fp64(gpu, kind, n):
+    # the precision form's triplets by FP32 FFT (round-to-nearest CUDA-core arithmetic): its
+    # iterations track FP64 as closely as the 3xTF32 dense passes do
+    from crysscft_sample_b200 import fields
+
+    N, L = (n, n, n), 4.2
+    wA, wB = fields.seed_fields(N, L, "BCC")
+    F = {}
+    for form, prec in (("dense", "fp64"), ("fft", "fp32"), ("dense", "fp32")):
+        with _Form(form):
+            G = solvers.make_solver(kind, N)
+            G.set_cell_para((L, L, L))
+            run = scft.DiblockSCFT(G, 0.25, 0.005, 20.0, 0.1)
+            run.set_fields(fields.to_physical(kind, wA), fields.to_physical(kind, wB))
+            run.set_precision(prec)
+            F[(form, prec)] = run.iterate(3)["F"]
+            run.close()
+            G.close()
+    ref64 = F[("dense", "fp64")]
+    rel_fft = np.abs(F[("fft", "fp32")] - ref64) / np.abs(ref64)
+    rel_tf32 = np.abs(F[("dense", "fp32")] - ref64) / np.abs(ref64)
+    print(f"\n{kind} {n}^3 FP32 |dF/F| vs FP64: FFT {rel_fft.max():.3e}, 3xTF32 dense {rel_tf32.max():.3e}")
+    assert 1e-12 < rel_fft.max() < 3e-5
+    assert not np.array_equal(F[("fft", "fp32")], F[("dense", "fp32")])
