@@ -178,6 +178,9 @@ __global__ void __launch_bounds__(kFftThreads) axis_fft_kernel(const AxisFftPass
     using S = FftShape<N, NF, EXT, R>;
     using Cx = typename CplxOf<R>::type;
     constexpr int T = S::T, LINES = S::LINES;
+    constexpr int PER = LINES * N / kFftThreads;  // tile values per thread
+    constexpr int CH = PER < 8 ? PER : 8;         // loads in flight per thread and chunk
+    static_assert(LINES * N % kFftThreads == 0 && PER % CH == 0, "whole chunks per thread");
     extern __shared__ __align__(16) unsigned char fft_raw[];
     __shared__ long long s_base[LINES];  // offset of element 0 of each line of the tile (-1: none)
     R* buf = reinterpret_cast<R*>(fft_raw);
@@ -213,24 +216,29 @@ __global__ void __launch_bounds__(kFftThreads) axis_fft_kernel(const AxisFftPass
             s_base[l] = b;
         }
         __syncthreads();
-        // load the tile (buf[l][j]), coalesced along j for contiguous lines, along l otherwise
-        for (int e = tid; e < LINES * N; e += kFftThreads) {
-            int l, j;
-            if (contiguous) {
-                l = e / N;
-                j = e - l * N;
-            } else {
-                j = e / LINES;
-                l = e - j * LINES;
-            }
-            const long long b = s_base[l];
-            R v = R(0);
-            if (b >= 0) {
+        // load the tile (buf[l][j]), coalesced along j for contiguous lines, along l otherwise;
+        // the loads of a chunk are all issued before its shared-memory stores, so their
+        // latencies overlap
+#pragma unroll 1
+        for (int k0 = 0; k0 < PER; k0 += CH) {
+            R v[CH], w[CH];
+#pragma unroll
+            for (int k = 0; k < CH; ++k) {
+                const int e = tid + (k0 + k) * kFftThreads;
+                const int l = contiguous ? e / N : e % LINES;
+                const int j = contiguous ? e % N : e / LINES;
+                const long long b = s_base[l];
                 const long long idx = b + (long long)j * inner;
-                v = in[idx];
-                if (pre) v *= pre[idx];
+                v[k] = b >= 0 ? __ldg(in + idx) : R(0);
+                w[k] = (b >= 0 && pre) ? __ldg(pre + idx) : R(1);
             }
-            buf[l * N + j] = v;
+#pragma unroll
+            for (int k = 0; k < CH; ++k) {
+                const int e = tid + (k0 + k) * kFftThreads;
+                const int l = contiguous ? e / N : e % LINES;
+                const int j = contiguous ? e % N : e / LINES;
+                buf[l * N + j] = v[k] * w[k];
+            }
         }
         __syncthreads();
         Cx z[16];
@@ -280,21 +288,24 @@ __global__ void __launch_bounds__(kFftThreads) axis_fft_kernel(const AxisFftPass
         __syncthreads();
         R* out = p.out[c];
         const R* post = p.post[c];
-        for (int e = tid; e < LINES * N; e += kFftThreads) {
-            int l, j;
-            if (contiguous) {
-                l = e / N;
-                j = e - l * N;
-            } else {
-                j = e / LINES;
-                l = e - j * LINES;
+#pragma unroll 1
+        for (int k0 = 0; k0 < PER; k0 += CH) {
+            R w[CH];
+#pragma unroll
+            for (int k = 0; k < CH; ++k) {
+                const int e = tid + (k0 + k) * kFftThreads;
+                const int l = contiguous ? e / N : e % LINES;
+                const int j = contiguous ? e % N : e / LINES;
+                const long long b = s_base[l];
+                w[k] = (b >= 0 && post) ? __ldg(post + b + (long long)j * inner) : R(1);
             }
-            const long long b = s_base[l];
-            if (b >= 0) {
-                const long long idx = b + (long long)j * inner;
-                R v = buf[l * N + j];
-                if (post) v *= post[idx];
-                out[idx] = v;
+#pragma unroll
+            for (int k = 0; k < CH; ++k) {
+                const int e = tid + (k0 + k) * kFftThreads;
+                const int l = contiguous ? e / N : e % LINES;
+                const int j = contiguous ? e % N : e / LINES;
+                const long long b = s_base[l];
+                if (b >= 0) out[b + (long long)j * inner] = buf[l * N + j] * w[k];
             }
         }
     }

@@ -42,14 +42,16 @@ def main(argv=None) -> int:
     if a.triplets:
         G.set_contour_step(a.ds)
         M = G.get_space_size_phy()
+        stream = torch.cuda.Stream()  # the solver's work and the timing events on one stream
+        G.set_stream(stream)
         q = torch.tensor(np.random.default_rng(1).random(M) + 0.5, dtype=torch.float64, device="cuda")
-        G.diffusion_device(q)
         torch.cuda.synchronize()
+        G.diffusion_device(q, stream)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
+        e0.record(stream)
         for _ in range(a.triplets):
-            G.diffusion_device(q, torch.cuda.current_stream())
-        e1.record()
+            G.diffusion_device(q, stream)
+        e1.record(stream)
         e1.synchronize()
         ms = e0.elapsed_time(e1) / a.triplets
         print(f"{a.triplets} triplets on {G.get_grid_size_phy()} physical: {ms * 1e3:.1f} us per triplet "
