@@ -310,8 +310,11 @@ AxisFftFn<R> axis_fft_kernel_for(int n, int nf, int ext, size_t* smem) {
     return nullptr;
 }
 
-// Which form runs the FP64 axis passes: CRYSSCFT_AXIS_FORM=fft or =dense forces one (for
-// measurements and tests); the default is the dense form.
+// Which form runs the per-axis passes: CRYSSCFT_AXIS_FORM=fft or =dense forces one (for
+// measurements and tests); by default the FFT passes run where no tensor-core axis kernel
+// covers the grid (the dense alternative is then the SIMT GEMM, e.g. 256-point P1 axes:
+// 2.99 ms against 0.50 ms per 256^3 triplet), the tensor-core passes where they exist
+// (128-point PMMM axes: 56 us against 97 us).
 int axis_form_override() {
     const char* e = getenv("CRYSSCFT_AXIS_FORM");
     return !e ? 0 : (e[0] == 'f' ? 1 : (e[0] == 'd' ? 2 : 0));
@@ -642,6 +645,23 @@ struct scft_solver_s {
     }
     std::vector<const void*> fft_fn_set;  // FFT kernels granted their dynamic shared memory
 
+    // whether the tensor-core axis passes (axis_dmma.cuh: FP64 DMMA; FP32: 3xTF32) cover this
+    // grid: cubic, one even/odd form on every axis, a side with a kernel (96 or 128)
+    template <typename T>
+    bool tensor_axis_passes() const {
+        const OpsSet* o = ops;
+        const int n = (int)grid_phy[0];
+        if (o->nterms != 1 || grid_phy[1] != grid_phy[0] || grid_phy[2] != grid_phy[0]) return false;
+        size_t smem = 0, stride = 0;
+        if constexpr (sizeof(T) == 8) {
+            if (o->eo[0] != o->eo[1] || o->eo[1] != o->eo[2]) return false;
+            return axis_dmma_kernel_for(n, o->eo[0], 2, &smem, o->eo2 && n == 128) != nullptr;
+        } else {
+            if (o->eo_f32[0] != o->eo_f32[1] || o->eo_f32[1] != o->eo_f32[2]) return false;
+            return axis_tf32_kernel_for(n, o->eo_f32[0], 2, &smem, &stride) != nullptr;
+        }
+    }
+
     // the three passes of a triplet by FFT (axis_fft.cuh); *done = false if an axis has no
     // FFT form or the dense form is to run
     template <typename T>
@@ -649,7 +669,9 @@ struct scft_solver_s {
         *done = false;
         const OpsSet* o = ops;
         if (o->nterms != 1) return SCFT_OK;
-        if (axis_form_override() != 1) return SCFT_OK;
+        const int form = axis_form_override();
+        if (form == 2) return SCFT_OK;
+        if (form == 0 && tensor_axis_passes<T>()) return SCFT_OK;  // measured faster where they exist
         AxisFftFn<T> f[3];
         size_t sm[3];
         for (int ax = 0; ax < 3; ++ax) {
