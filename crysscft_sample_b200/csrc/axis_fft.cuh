@@ -51,7 +51,8 @@ struct FftShape {
     static constexpr int PAIRS = kFftThreads / T;
     static constexpr int LINES = 2 * PAIRS;
     static constexpr int XROW = T + 1;              // exchange row (padded against bank conflicts)
-    static constexpr size_t TILE_BYTES = (size_t)LINES * N * sizeof(R);
+    static constexpr int LS = N + 1;                // tile line stride: lines along l hit distinct banks
+    static constexpr size_t TILE_BYTES = (size_t)LINES * LS * sizeof(R);
     static constexpr size_t XCH_BYTES = (size_t)PAIRS * 16 * XROW * 2 * sizeof(R);
     static constexpr size_t BUF_BYTES = TILE_BYTES > XCH_BYTES ? TILE_BYTES : XCH_BYTES;
     static constexpr size_t SMEM = BUF_BYTES + (size_t)NF * 3 * sizeof(R);
@@ -177,7 +178,7 @@ template <int N, int NF, int EXT, typename R = double>
 __global__ void __launch_bounds__(kFftThreads) axis_fft_kernel(const AxisFftPass<R> p) {
     using S = FftShape<N, NF, EXT, R>;
     using Cx = typename CplxOf<R>::type;
-    constexpr int T = S::T, LINES = S::LINES;
+    constexpr int T = S::T, LINES = S::LINES, LS = S::LS;
     constexpr int PER = LINES * N / kFftThreads;  // tile values per thread
     constexpr int CH = PER < 8 ? PER : 8;         // loads in flight per thread and chunk
     static_assert(LINES * N % kFftThreads == 0 && PER % CH == 0, "whole chunks per thread");
@@ -237,13 +238,13 @@ __global__ void __launch_bounds__(kFftThreads) axis_fft_kernel(const AxisFftPass
                 const int e = tid + (k0 + k) * kFftThreads;
                 const int l = contiguous ? e / N : e % LINES;
                 const int j = contiguous ? e % N : e / LINES;
-                buf[l * N + j] = v[k] * w[k];
+                buf[l * LS + j] = v[k] * w[k];
             }
         }
         __syncthreads();
         Cx z[16];
-        const R* l1 = buf + (2 * pair) * N;
-        const R* l2 = l1 + N;
+        const R* l1 = buf + (2 * pair) * LS;
+        const R* l2 = l1 + LS;
 #pragma unroll
         for (int m = 0; m < 16; ++m) {
             const int k = T * m + t;
@@ -265,8 +266,8 @@ __global__ void __launch_bounds__(kFftThreads) axis_fft_kernel(const AxisFftPass
         }
         fft_pair<NF>(z, my, stw, t);
         // results: A x1 = Re, A x2 = -Im, at the kept points of the extension
-        R* o1 = buf + (2 * pair) * N;
-        R* o2 = o1 + N;
+        R* o1 = buf + (2 * pair) * LS;
+        R* o2 = o1 + LS;
 #pragma unroll
         for (int m = 0; m < 16; ++m) {
             const int k = T * m + t;
@@ -305,7 +306,7 @@ __global__ void __launch_bounds__(kFftThreads) axis_fft_kernel(const AxisFftPass
                 const int l = contiguous ? e / N : e % LINES;
                 const int j = contiguous ? e % N : e / LINES;
                 const long long b = s_base[l];
-                if (b >= 0) out[b + (long long)j * inner] = buf[l * N + j] * w[k];
+                if (b >= 0) out[b + (long long)j * inner] = buf[l * LS + j] * w[k];
             }
         }
     }
