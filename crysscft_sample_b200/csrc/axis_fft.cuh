@@ -158,8 +158,16 @@ __device__ __forceinline__ void fft_pair(Cx (&z)[16], Cx* xch, const Cx* tw, int
     constexpr int T = NF / 16, XROW = T + 1, C = 16 / T;
     Cx y[16];
     dft16(z, y);  // y[k1] = sum_{n1} x[T n1 + t] W16^(n1 k1)
+    // twiddles W_NF^(t k1) as a running product of W_NF^t (one table read per thread: the
+    // strided reads tw[t k1] collided on the shared-memory banks); <= 15 products, ~1e-15
+    const Cx wt = tw[t];
+    Cx w = wt;
+    xch[t] = y[0];
 #pragma unroll
-    for (int k1 = 0; k1 < 16; ++k1) xch[k1 * XROW + t] = k1 && t ? cmul(y[k1], tw[t * k1]) : y[k1];
+    for (int k1 = 1; k1 < 16; ++k1) {
+        xch[k1 * XROW + t] = cmul(y[k1], w);
+        w = cmul(w, wt);
+    }
     __syncthreads();
 #pragma unroll
     for (int c = 0; c < C; ++c) {
