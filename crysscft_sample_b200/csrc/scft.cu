@@ -311,10 +311,10 @@ AxisFftFn<R> axis_fft_kernel_for(int n, int nf, int ext, size_t* smem) {
 }
 
 // Which form runs the per-axis passes: CRYSSCFT_AXIS_FORM=fft or =dense forces one (for
-// measurements and tests); by default the FFT passes run where no tensor-core axis kernel
-// covers the grid (the dense alternative is then the SIMT GEMM, e.g. 256-point P1 axes:
-// 2.99 ms against 0.50 ms per 256^3 triplet), the tensor-core passes where they exist
-// (128-point PMMM axes: 56 us against 97 us).
+// measurements and tests); by default the FFT passes run wherever they exist except for
+// PMMM grids that the tensor-core passes cover (scft_solver_s::tensor_axis_passes).  Per
+// triplet on one B200: 256-point P1 axes 0.28 ms by FFT against 2.99 ms by the SIMT GEMMs;
+// 128-point PMMM axes 65 us by FFT against 56 us by DMMA.
 int axis_form_override() {
     const char* e = getenv("CRYSSCFT_AXIS_FORM");
     return !e ? 0 : (e[0] == 'f' ? 1 : (e[0] == 'd' ? 2 : 0));
@@ -645,12 +645,16 @@ struct scft_solver_s {
     }
     std::vector<const void*> fft_fn_set;  // FFT kernels granted their dynamic shared memory
 
-    // whether the tensor-core axis passes (axis_dmma.cuh: FP64 DMMA; FP32: 3xTF32) cover this
-    // grid: cubic, one even/odd form on every axis, a side with a kernel (96 or 128)
+    // whether the tensor-core axis passes (axis_dmma.cuh: FP64 DMMA; FP32: 3xTF32) run this
+    // grid by default: PMMM (its two-level even/odd operators) on a cubic grid with a side the
+    // kernels cover (96 or 128); measured per 256^3 triplet: 56 us against 65 us by FFT, while
+    // for P1 and 3m the FFT passes are faster (128-point P1 axes 50 against 58 us, 128-point 3m
+    // axes 68 against 82 us)
     template <typename T>
     bool tensor_axis_passes() const {
         const OpsSet* o = ops;
         const int n = (int)grid_phy[0];
+        if (kind != SCFT_SOLVER_PMMM) return false;
         if (o->nterms != 1 || grid_phy[1] != grid_phy[0] || grid_phy[2] != grid_phy[0]) return false;
         size_t smem = 0, stride = 0;
         if constexpr (sizeof(T) == 8) {
