@@ -55,7 +55,7 @@ struct FftShape {
     static constexpr size_t TILE_BYTES = (size_t)LINES * LS * sizeof(R);
     static constexpr size_t XCH_BYTES = (size_t)PAIRS * 16 * XROW * 2 * sizeof(R);
     static constexpr size_t BUF_BYTES = TILE_BYTES > XCH_BYTES ? TILE_BYTES : XCH_BYTES;
-    static constexpr size_t SMEM = BUF_BYTES;  // the twiddle and spectrum tables are read through L1
+    static constexpr size_t SMEM = BUF_BYTES + (size_t)NF * 3 * sizeof(R);
 };
 
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
@@ -152,7 +152,7 @@ __device__ __forceinline__ void dft_small(C* x) {
 }
 
 // NF-point forward FFT of one line pair, z[m] = x[T m + t] in, X[T m + t] out.
-// xch: this pair's exchange rows (16 x XROW), tw: the NF twiddles (global memory, read once).
+// xch: this pair's exchange rows (16 x XROW), tw: the NF twiddles (shared memory).
 template <int NF, typename Cx>
 __device__ __forceinline__ void fft_pair(Cx (&z)[16], Cx* xch, const Cx* tw, int t) {
     constexpr int T = NF / 16, XROW = T + 1, C = 16 / T;
@@ -160,7 +160,7 @@ __device__ __forceinline__ void fft_pair(Cx (&z)[16], Cx* xch, const Cx* tw, int
     dft16(z, y);  // y[k1] = sum_{n1} x[T n1 + t] W16^(n1 k1)
     // twiddles W_NF^(t k1) as a running product of W_NF^t (one table read per thread: the
     // strided reads tw[t k1] collided on the shared-memory banks); <= 15 products, ~1e-15
-    const Cx wt = __ldg(tw + t);
+    const Cx wt = tw[t];
     Cx w = wt;
     xch[t] = y[0];
 #pragma unroll
@@ -183,7 +183,7 @@ __device__ __forceinline__ void fft_pair(Cx (&z)[16], Cx* xch, const Cx* tw, int
 }
 
 template <int N, int NF, int EXT, typename R = double>
-__global__ void __launch_bounds__(kFftThreads, 3) axis_fft_kernel(const AxisFftPass<R> p) {
+__global__ void __launch_bounds__(kFftThreads) axis_fft_kernel(const AxisFftPass<R> p) {
     using S = FftShape<N, NF, EXT, R>;
     using Cx = typename CplxOf<R>::type;
     constexpr int T = S::T, LINES = S::LINES, LS = S::LS;
@@ -194,9 +194,13 @@ __global__ void __launch_bounds__(kFftThreads, 3) axis_fft_kernel(const AxisFftP
     __shared__ long long s_base[LINES];  // offset of element 0 of each line of the tile (-1: none)
     R* buf = reinterpret_cast<R*>(fft_raw);
     Cx* xch = reinterpret_cast<Cx*>(fft_raw);  // aliases the tile between its uses
-    const Cx* stw = p.tw;  // one value per thread and transform (running product, fft_pair)
-    const R* sg = p.g;     // 16 values per thread and tile
+    Cx* stw = reinterpret_cast<Cx*>(fft_raw + S::BUF_BYTES);
+    R* sg = reinterpret_cast<R*>(stw + NF);
     const int tid = threadIdx.x;
+    for (int e = tid; e < NF; e += kFftThreads) {
+        stw[e] = p.tw[e];
+        sg[e] = p.g[e];
+    }
     const int pair = tid / T, t = tid - (tid / T) * T;
     const long long lines = p.outer * p.inner;  // per chain
     const long long tiles_per_chain = (lines + LINES - 1) / LINES;
@@ -264,7 +268,7 @@ __global__ void __launch_bounds__(kFftThreads, 3) axis_fft_kernel(const AxisFftP
         fft_pair<NF>(z, my, stw, t);
 #pragma unroll
         for (int m = 0; m < 16; ++m) {
-            const R gk = __ldg(sg + T * m + t);
+            const R gk = sg[T * m + t];
             z[m].x = z[m].x * gk;
             z[m].y = -z[m].y * gk;
         }
