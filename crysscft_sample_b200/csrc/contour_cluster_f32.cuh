@@ -367,9 +367,12 @@ __global__ void __launch_bounds__(kClThreads, 1) contour_cluster_kernel_f32(cons
         }
         // ---- D, store q(j), D
         if (!failed) {
-            if (!mbar_wait(&s_bar_d, dph, a.spin_limit)) bad = true;
-            if (tid == 0) d_pending = false;
-            dph ^= 1u;
+            if (mbar_wait(&s_bar_d, dph, a.spin_limit)) {
+                if (tid == 0) d_pending = false;  // a copy that did not land is drained at exit
+                dph ^= 1u;
+            } else {
+                bad = true;
+            }
         }
         if (!failed && !bad) {
             const int bcur = j >= 1 ? cl_block_of(slot0, dir, a.NsA, j - 1) : -1;

@@ -42,6 +42,39 @@ def test_a_wait_that_runs_out_is_a_timeout_and_the_context_survives(gpu, precisi
     assert np.array_equal(got, want)
 
 
+def test_cluster_kernel_timeout_drains_and_the_context_survives(gpu, monkeypatch):
+    # the FP32 cluster kernel (tcgen05 MMAs, bulk copies, cluster barriers): a wait that runs
+    # out makes every CTA skip its work but keep the cluster barriers, drain its own MMAs and
+    # copies, free its tensor memory and return; the call reports SCFT_ERR_TIMEOUT and the
+    # context then reproduces a fresh run
+    monkeypatch.setenv("CRYSSCFT_FP32_CLUSTER", "1")
+    n = (128, 128, 128)  # 64^3 physical: the grid the cluster kernel runs
+    wA, wB = fields.seed_fields(n, L, "BCC")
+    a, b = fields.to_physical("PMMM", wA), fields.to_physical("PMMM", wB)
+
+    def fresh():
+        G = solvers.make_solver("PMMM", n)
+        G.set_cell_para((L, L, L))
+        r = scft.DiblockSCFT(G, 0.25, 0.01, 20.0, 0.1)
+        r.set_fields(a, b)
+        r.set_precision("fp32")
+        return r
+
+    want = fresh().iterate(2)["F"]
+    monkeypatch.setenv("CRYSSCFT_FP32_CLUSTER", "0")
+    assert not np.array_equal(fresh().iterate(2)["F"], want)  # the cluster kernel really ran
+    monkeypatch.setenv("CRYSSCFT_FP32_CLUSTER", "1")
+    run = fresh()
+    run.iterate(1)
+    run.set_wait_limit(1)
+    with pytest.raises(ScftError) as e:
+        run.iterate(1)
+    assert e.value.status == 7  # SCFT_ERR_TIMEOUT
+    run.set_wait_limit()
+    run.set_fields(a, b)
+    assert np.array_equal(run.iterate(2)["F"], want)
+
+
 def test_non_finite_fields_are_a_numeric_error(gpu):
     run, a, b = _fresh()
     bad = a.copy()
