@@ -75,6 +75,23 @@ __device__ __forceinline__ void mma_f16_ts(unsigned d, unsigned a, unsigned long
         "r"(a), "l"(bdesc), "r"(accumulate), "r"(kIdesc)
         : "memory");
 }
+// Bounded wait on an mbarrier phase with the non-blocking test (try_wait may suspend the
+// thread for a hardware-chosen time inside one poll, so a poll count would not bound the
+// wait's length, and a limit of one poll would not reliably run out)
+__device__ __forceinline__ bool cl_mbar_wait(unsigned long long* bar, unsigned parity, long long limit) {
+    long long spins = 0;
+    for (;;) {
+        unsigned ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+            : "=r"(ok)
+            : "r"(smem_u32(bar)), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        if (++spins > limit) return false;
+        if (spins > 64) __nanosleep(20);
+    }
+}
 __device__ __forceinline__ void mma_commit(unsigned long long* bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                  : "memory");
@@ -227,16 +244,7 @@ __device__ __forceinline__ bool cl_axis_op(float (&v)[64], const __half* opaxis,
         }
     }
     // wait for this block's products (bounded)
-    bool ok = true;
-    {
-        long long spins = 0;
-        while (!mbar_test(&o.bar[blk], ph[blk])) {
-            if (++spins > o.limit) {
-                ok = false;
-                break;
-            }
-        }
-    }
+    const bool ok = cl_mbar_wait(&o.bar[blk], ph[blk], o.limit);
     ph[0] ^= 1u;
     ph[1] ^= 1u;
     if (!ok) return false;
@@ -367,7 +375,7 @@ __global__ void __launch_bounds__(kClThreads, 1) contour_cluster_kernel_f32(cons
         }
         // ---- D, store q(j), D
         if (!failed) {
-            if (mbar_wait(&s_bar_d, dph, a.spin_limit)) {
+            if (cl_mbar_wait(&s_bar_d, dph, a.spin_limit)) {
                 if (tid == 0) d_pending = false;  // a copy that did not land is drained at exit
                 dph ^= 1u;
             } else {
