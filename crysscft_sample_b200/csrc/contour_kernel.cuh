@@ -73,13 +73,6 @@ struct ContourArgs {
     // as (z % 8, row, z / 8, tile)
     alignas(64) CUtensorMap tm_pq[2][2];
     alignas(64) CUtensorMap tm_pw[2][2];
-    // alternating kernel, blocks after the units (0 helpers: none): the contour integral of
-    // the densities over the interior slots s = 1..U-1 while the chains run.  done[chain][phase]
-    // counts the units whose q store of that phase has landed (zeroed by the host); phi_raw
-    // receives [A | B] sums of w_s q(s) q+(s) (trapezoid weights 1/2 or 1, no 1/(Ns Q))
-    unsigned* done;
-    double* phi_raw;
-    int helpers;
 };
 
 __device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
@@ -943,144 +936,6 @@ __device__ __forceinline__ int tma_alignment_error(const void* const* tiles, int
     return e;
 }
 
-__device__ __forceinline__ void red_release_add_u32(unsigned* p, unsigned v) {
-    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-// bulk-copy (async proxy) writes to global memory, complete, ordered before the generic
-// accesses and releases that follow
-__device__ __forceinline__ void fence_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
-
-// Trapezoid weight of contour slot s in the block covering slots [lo, hi]: 1/2 at the ends,
-// 1 inside, 0 outside (the rule of src/crysSCFT_sample.cpp:348-360 without its 1/Ns)
-__device__ __forceinline__ double phi_weight(long long s, long long lo, long long hi) {
-    return (s < lo || s > hi) ? 0.0 : ((s == lo || s == hi) ? 0.5 : 1.0);
-}
-
-// Helper block h of the alternating kernel: accumulates phi over the slots s = 1..U-1 for a
-// contiguous range of points, in shared memory, while the units run the chains.  Slot s is
-// complete once the forward chain has stored it (phase s) and the backward chain has
-// stored it (phase U - s), i.e. at phase t = max(s, U - s): the helper walks t = ceil(U/2) ..
-// U - 1 and adds the pairs s = t and s = U - t as their stores land.  Slots 0 and U (complete
-// only when the launch ends) and the 1/(Ns Q) factors are left to the kernel that follows.
-// The order of the additions per point is fixed (t ascending), so the result does not depend
-// on timing.
-template <int UNR>
-__device__ void phi_helper(const ContourArgs& a, int h, unsigned units_per_chain, long long M, double* acc) {
-    const int U = a.t_end;
-    const long long per = ((M / 2 + a.helpers - 1) / a.helpers) * 2;  // points per helper (even)
-    const long long b0 = (long long)h * per;
-    const long long b1 = b0 + per < M ? b0 + per : M;
-    const long long n2 = b1 > b0 ? (b1 - b0) / 2 : 0;  // double2 positions of this helper
-    double2* accA = reinterpret_cast<double2*>(acc);
-    double2* accB = accA + per / 2;
-    for (long long j = threadIdx.x; j < n2; j += kContourThreads) {
-        accA[j] = make_double2(0.0, 0.0);
-        accB[j] = make_double2(0.0, 0.0);
-    }
-    __shared__ int s_go;
-    const double* q = a.q[0];
-    const double* qc = a.q[1];
-    for (int t = (U + 1) / 2; t <= U - 1; ++t) {
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int ok = 1;
-            long long spins = 0;
-            const unsigned* d0 = a.done + t;
-            const unsigned* d1 = a.done + (U + 1) + t;
-            while (ld_acquire_u32(d0) < units_per_chain || ld_acquire_u32(d1) < units_per_chain) {
-                if (*((volatile int*)a.error) != 0) {  // a unit gave up: leave without waiting
-                    ok = 0;
-                    break;
-                }
-                if (++spins > a.spin_limit) {
-                    atomicOr(a.error, 1);
-                    ok = 0;
-                    break;
-                }
-                if (spins > 64) __nanosleep(64);
-            }
-            s_go = ok;
-        }
-        __syncthreads();
-        if (!s_go) return;
-        const long long s1 = t, s2 = U - t;
-        const bool two = s2 != s1;
-        const double wa1 = phi_weight(s1, 0, a.NsA), wb1 = phi_weight(s1, a.NsA, U);
-        const double wa2 = two ? phi_weight(s2, 0, a.NsA) : 0.0, wb2 = two ? phi_weight(s2, a.NsA, U) : 0.0;
-        const double2* x1p = reinterpret_cast<const double2*>(q + s1 * M + b0);
-        const double2* y1p = reinterpret_cast<const double2*>(qc + s1 * M + b0);
-        const double2* x2p = reinterpret_cast<const double2*>(q + s2 * M + b0);
-        const double2* y2p = reinterpret_cast<const double2*>(qc + s2 * M + b0);
-        for (long long j0 = threadIdx.x; j0 < n2; j0 += UNR * kContourThreads) {
-            double2 x1[UNR], y1[UNR], x2[UNR], y2[UNR];
-#pragma unroll
-            for (int r = 0; r < UNR; ++r) {  // every load of the round in flight together
-                const long long j = j0 + (long long)r * kContourThreads;
-                x1[r] = y1[r] = x2[r] = y2[r] = make_double2(0.0, 0.0);
-                if (j < n2) {
-                    x1[r] = __ldcg(x1p + j);
-                    y1[r] = __ldcg(y1p + j);
-                    if (two) {
-                        x2[r] = __ldcg(x2p + j);
-                        y2[r] = __ldcg(y2p + j);
-                    }
-                }
-            }
-#pragma unroll
-            for (int r = 0; r < UNR; ++r) {
-                const long long j = j0 + (long long)r * kContourThreads;
-                if (j < n2) {
-                    const double p1x = x1[r].x * y1[r].x, p1y = x1[r].y * y1[r].y;
-                    const double p2x = x2[r].x * y2[r].x, p2y = x2[r].y * y2[r].y;
-                    double2 va = accA[j], vb = accB[j];
-                    va.x += wa1 * p1x + wa2 * p2x;
-                    va.y += wa1 * p1y + wa2 * p2y;
-                    vb.x += wb1 * p1x + wb2 * p2x;
-                    vb.y += wb1 * p1y + wb2 * p2y;
-                    accA[j] = va;
-                    accB[j] = vb;
-                }
-            }
-        }
-    }
-    __syncthreads();
-    double2* oA = reinterpret_cast<double2*>(a.phi_raw + b0);
-    double2* oB = reinterpret_cast<double2*>(a.phi_raw + M + b0);
-    for (long long j = threadIdx.x; j < n2; j += kContourThreads) {
-        oA[j] = accA[j];
-        oB[j] = accB[j];
-    }
-}
-
-// phi after a launch with helper blocks: their interior sums plus the end slots 0 and U,
-// times fA / (NsA Q) and fB / (NsB Q) (src/crysSCFT_sample.cpp:348-360); M even
-__global__ void phi_finish_kernel(const double* __restrict__ q, const double* __restrict__ qc,
-                                  const double* __restrict__ raw, double* __restrict__ phiA,
-                                  double* __restrict__ phiB, const double* Qp, double fA, long long NsA,
-                                  long long NsB, long long M) {
-    const long long U = NsA + NsB;
-    const double Q = *Qp;
-    const double cA = fA / (NsA * Q);
-    const double cB = (1 - fA) / (NsB * Q);
-    const double wa0 = phi_weight(0, 0, NsA), waU = phi_weight(U, 0, NsA);
-    const double wb0 = phi_weight(0, NsA, U), wbU = phi_weight(U, NsA, U);
-    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < M / 2;
-         j += (long long)gridDim.x * blockDim.x) {
-        const long long i = 2 * j;
-        const double2 x0 = __ldcs(reinterpret_cast<const double2*>(q + i));
-        const double2 y0 = __ldcs(reinterpret_cast<const double2*>(qc + i));
-        const double2 xU = __ldcs(reinterpret_cast<const double2*>(q + U * M + i));
-        const double2 yU = __ldcs(reinterpret_cast<const double2*>(qc + U * M + i));
-        const double2 ra = *reinterpret_cast<const double2*>(raw + i);
-        const double2 rb = *reinterpret_cast<const double2*>(raw + M + i);
-        const double p0x = x0.x * y0.x, p0y = x0.y * y0.y, pUx = xU.x * yU.x, pUy = xU.y * yU.y;
-        *reinterpret_cast<double2*>(phiA + i) =
-            make_double2(cA * (ra.x + wa0 * p0x + waU * pUx), cA * (ra.y + wa0 * p0y + waU * pUy));
-        *reinterpret_cast<double2*>(phiB + i) =
-            make_double2(cB * (rb.x + wb0 * p0x + wbU * pUx), cB * (rb.y + wb0 * p0y + wbU * pUy));
-    }
-}
-
 template <int N, bool EO, bool EO2 = false>
 __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const __grid_constant__ ContourArgs a) {
     static_assert(!EO2 || (EO && N == 64), "two even/odd levels: n = 64");
@@ -1112,10 +967,7 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
         if (threadIdx.x == 0) atomicOr(a.error, 4);
         return;
     }
-    if (u >= units) {
-        if (u - units < a.helpers) phi_helper<8>(a, u - units, (unsigned)N, M, smem);
-        return;
-    }
+    if (u >= units) return;
     const int warp = threadIdx.x >> 5;
     {
         const void* tiles[3] = {W0, W1, QS};
@@ -1190,13 +1042,6 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
         const bool plane = (k & 1) == 0;
         const long long off = plane ? (long long)p * PLANE : (long long)p * N;
         const long long gs = plane ? N : PLANE;
-        if (a.helpers && k >= 2 && threadIdx.x == 0) {
-            // the q store of phase k-1 (this thread's only bulk group) has landed: count it
-            // for the helpers (off the critical path: the exchange wait follows)
-            bulk_wait_all();
-            fence_async_global();
-            red_release_add_u32(a.done + (size_t)c * (U + 1) + (k - 1), 1u);
-        }
         if (k == 0) {
             tile_fetch<N, LF>(T0, q + slot0 * M + off, gs);
         } else {

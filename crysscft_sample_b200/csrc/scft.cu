@@ -993,11 +993,6 @@ struct scft_diblock_s {
     int last_form = 0;                    // force_form the current launch plan was built with
     DevBuf<double> d_xch;                 // exchange buffers, 2 x space_size_phy per chain
     DevBuf<unsigned> flags;               // per-unit phase flags of the alternating kernel
-    // FP64 alternating kernel: blocks after the units accumulate phi while the chains run
-    // (phi_helper); the batch runs instances concurrently and keeps the separate phi pass
-    bool allow_phi_helpers = true;
-    int phi_helpers = 0;
-    DevBuf<double> phi_raw;               // [A | B] x M interior sums of the helpers
     int last_iter_precision = -1;         // precision of the iteration whose contour is stored
     DevBuf<double> stress_buf;            // batched temporaries of scft_diblock_stress
     ContourFnF contour_fn_f32 = nullptr;  // FP32 (3xTF32) contour kernel
@@ -1099,11 +1094,6 @@ struct scft_diblock_s {
         return SCFT_OK;
     }
 
-    // phase flags of the alternating kernels: 4 n^2 exchange flags, then the helpers' 2 (U + 1)
-    // store counters; one size for both precisions, so that switching never reallocates
-    // the buffer under the other precision's captured graph
-    size_t flags_count(int nx) const { return (size_t)4 * nx * nx + 2 * (U + 1); }
-
     int setup_persistent_f32() {
         persistent = false;
         CKR(setup_cluster_f32());
@@ -1128,7 +1118,7 @@ struct scft_diblock_s {
         persistent_grid = 2 * nx;
         persistent_smem = smem;
         if (!f_xch.p) CKR(f_xch.alloc(4 * M));
-        if (flags.n != flags_count(nx)) CKR(flags.alloc(flags_count(nx)));
+        if (flags.n != (size_t)(4 * nx * nx)) CKR(flags.alloc((size_t)4 * nx * nx));
         if (!ctrl.p) {
             CKR(ctrl.alloc(2));
             CK(cudaMemset(ctrl.p, 0, 2 * sizeof(unsigned)));
@@ -1215,6 +1205,7 @@ struct scft_diblock_s {
             }
         }
         if (!d_xch.p) CKR(d_xch.alloc(4 * M));
+        if (alternating && flags.n != (size_t)(4 * nx * nx)) CKR(flags.alloc((size_t)4 * nx * nx));
         CK(cudaFuncSetAttribute(contour_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 0;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, contour_fn, kContourThreads, smem));
@@ -1223,33 +1214,6 @@ struct scft_diblock_s {
         if (alternating && units > per_sm * sms) return SCFT_OK;  // one unit per block: per-axis kernels
         persistent_grid = std::min(units, per_sm * sms);
         persistent_smem = smem;
-        // phi helpers on the SMs the units leave free (one block per SM: the default; with
-        // CRYSSCFT_PHI_HELPERS=1 also where blocks would share SMs, =0 never); each keeps
-        // its range of points' two sums in shared memory
-        phi_helpers = 0;
-        if (alternating && allow_phi_helpers && M % 2 == 0) {
-            const char* e = getenv("CRYSSCFT_PHI_HELPERS");
-            const bool off = e && e[0] == '0', force = e && e[0] == '1';
-            const int room = std::min(per_sm * sms - units, sms);
-            if (!off && room > 0 && (per_sm == 1 || force)) {
-                const size_t per = ((M / 2 + (size_t)room - 1) / (size_t)room) * 2;
-                const size_t need = std::max(smem, 2 * per * sizeof(double) + 128);
-                int per_sm2 = 0;
-                if (need <= (size_t)dev_smem) {
-                    CK(cudaFuncSetAttribute(contour_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
-                    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, contour_fn, kContourThreads, need));
-                }
-                if (per_sm2 >= 1 && units + room <= per_sm2 * sms) {
-                    if (phi_raw.n != 2 * M) CKR(phi_raw.alloc(2 * M));
-                    phi_helpers = room;
-                    persistent_grid = units + room;
-                    persistent_smem = need;
-                } else {
-                    CK(cudaFuncSetAttribute(contour_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-                }
-            }
-        }
-        if (alternating && flags.n != flags_count(nx)) CKR(flags.alloc(flags_count(nx)));
         if (!ctrl.p) {
             CKR(ctrl.alloc(2));
             CK(cudaMemset(ctrl.p, 0, 2 * sizeof(unsigned)));
@@ -1288,11 +1252,6 @@ struct scft_diblock_s {
         a.error = reinterpret_cast<int*>(ctrl.p + 1);
         a.spin_limit = spin_limit;
         a.flags = flags.p;
-        if (alternating && phi_helpers) {
-            a.done = flags.p + (size_t)4 * solver->grid_phy[0] * solver->grid_phy[0];
-            a.phi_raw = phi_raw.p;
-            a.helpers = phi_helpers;
-        }
         CK(cudaMemsetAsync(ctrl.p, 0, sizeof(unsigned), st));
         if (alternating) {
             const int n = (int)solver->grid_phy[0];
@@ -1351,18 +1310,8 @@ struct scft_diblock_s {
         const int rblocks = (int)std::min<long long>(kRedMaxBlocks, (MM + kRedThreads - 1) / kRedThreads);
         q_reduce_kernel<T><<<rblocks, kRedThreads, 0, st>>>(qc, MM, partials.p, state.p);
         CK(cudaGetLastError());
-        bool phi_done = false;
-        if constexpr (sizeof(T) == 8) {
-            if (persistent && phi_helpers) {  // the contour launch summed the interior slots
-                phi_finish_kernel<<<grid_blocks(MM / 2, 256), 256, 0, st>>>(q, qc, phi_raw.p, phiA.p, phiB.p,
-                                                                           &state.p->Q, fA, (long long)NsA,
-                                                                           (long long)NsB, MM);
-                phi_done = true;
-            }
-        }
-        if (!phi_done)
-            phi_kernel<T><<<grid_blocks((MM + 1) / 2, 256), 256, 0, st>>>(q, qc, phiA.p, phiB.p, state.p, fA,
-                                                                          (long long)NsA, (long long)NsB, MM);
+        phi_kernel<T><<<grid_blocks((MM + 1) / 2, 256), 256, 0, st>>>(q, qc, phiA.p, phiB.p, state.p, fA, (long long)NsA,
+                                              (long long)NsB, MM);
         CK(cudaGetLastError());
         if (phase_events) CK(cudaEventRecord(phase_events[3], st));
         energy_kernel<<<rblocks, kRedThreads, 0, st>>>(wA.p, wB.p, phiA.p, phiB.p, ksi.p, xN, MM,
@@ -2256,7 +2205,6 @@ struct scft_batch_s {
         drop_graph();
         for (auto d : runs) {
             d->force_form = form;
-            d->allow_phi_helpers = false;
             if (d->captured_gen == d->solver->ops_gen && d->last_form != form) d->captured_gen = ~0ULL;
             d->last_form = form;
             CKR(diblock_prepare(d, false));
