@@ -311,10 +311,11 @@ AxisFftFn<R> axis_fft_kernel_for(int n, int nf, int ext, size_t* smem) {
 }
 
 // Which form runs the per-axis passes: CRYSSCFT_AXIS_FORM=fft or =dense forces one (for
-// measurements and tests); by default the FFT passes run wherever they exist except for
-// PMMM grids that the tensor-core passes cover (scft_solver_s::tensor_axis_passes).  Per
-// triplet on one B200: 256-point P1 axes 0.28 ms by FFT against 2.99 ms by the SIMT GEMMs;
-// 128-point PMMM axes 65 us by FFT against 56 us by DMMA.
+// measurements and tests); by default the FFT passes run wherever they exist except where
+// the tensor-core passes were measured faster (scft_solver_s::tensor_axis_passes: PMMM
+// grids they cover, and P1 iterations).  Per triplet on one B200: 256-point P1 axes 0.28 ms
+// by FFT against 2.99 ms by the SIMT GEMMs; 128-point PMMM axes 65 us by FFT against 56 us
+// by DMMA.
 int axis_form_override() {
     const char* e = getenv("CRYSSCFT_AXIS_FORM");
     return !e ? 0 : (e[0] == 'f' ? 1 : (e[0] == 'd' ? 2 : 0));
@@ -646,15 +647,17 @@ struct scft_solver_s {
     std::vector<const void*> fft_fn_set;  // FFT kernels granted their dynamic shared memory
 
     // whether the tensor-core axis passes (axis_dmma.cuh: FP64 DMMA; FP32: 3xTF32) run this
-    // grid by default: PMMM (its two-level even/odd operators) on a cubic grid with a side the
-    // kernels cover (96 or 128); measured per 256^3 triplet: 56 us against 65 us by FFT, while
-    // for P1 and 3m the FFT passes are faster (128-point P1 axes 50 against 58 us, 128-point 3m
-    // axes 68 against 82 us)
+    // grid by default, on a cubic grid with a side the kernels cover (96 or 128), from
+    // measurements on one B200: PMMM (two-level even/odd operators) always, 56 us against 65 us
+    // by FFT per 256^3 triplet; P1 for both chains of an iteration (128^3: 52.5 against 49.4
+    // iterations/s, precision form 69.7 against 62.1) but not for one chain (50 us by FFT
+    // against 58 us); never 3m (128-point axes: 68 us by FFT against 82 us per triplet, 36.6
+    // against 33.6 iterations/s at 256^3)
     template <typename T>
-    bool tensor_axis_passes() const {
+    bool tensor_axis_passes(int nchain) const {
         const OpsSet* o = ops;
         const int n = (int)grid_phy[0];
-        if (kind != SCFT_SOLVER_PMMM) return false;
+        if (kind == SCFT_SOLVER_3M || (kind == SCFT_SOLVER_P1 && nchain < 2)) return false;
         if (o->nterms != 1 || grid_phy[1] != grid_phy[0] || grid_phy[2] != grid_phy[0]) return false;
         size_t smem = 0, stride = 0;
         if constexpr (sizeof(T) == 8) {
@@ -675,7 +678,7 @@ struct scft_solver_s {
         if (o->nterms != 1) return SCFT_OK;
         const int form = axis_form_override();
         if (form == 2) return SCFT_OK;
-        if (form == 0 && tensor_axis_passes<T>()) return SCFT_OK;  // measured faster where they exist
+        if (form == 0 && tensor_axis_passes<T>(nchain)) return SCFT_OK;  // measured faster there
         AxisFftFn<T> f[3];
         size_t sm[3];
         for (int ax = 0; ax < 3; ++ax) {
