@@ -508,6 +508,7 @@ def run_batch(args):
     B = batch.BatchSCFT("PMMM", mine, ds=ds, precision="fp64", device=local)
     B.seed_fields()
     tuned = B.autotune(2)
+    plan = B.team_plan()  # the one-launch form's plan (grid 0 when another form was faster)
     B.iterate(max(args.warmup, 3))
     replicas.barrier(dist)
     torch.cuda.synchronize()
@@ -551,7 +552,8 @@ def run_batch(args):
             "triplets_per_s": trip * args.steps / dt,
             "config": {"workload": f"{args.instances} PMMM instances, reduced grids from {{16,24,32,48,64}}^3, "
                                    "chiN~U[14,30], fA~U[0.2,0.35], L~U[3.8,5.5], ds=0.01, BCC or FCC",
-                       "autotuned": tuned, "parallelism": f"instances sharded over {world} GPU(s)",
+                       "autotuned": tuned, "team_plan": plan,
+                       "parallelism": f"instances sharded over {world} GPU(s)",
                        "l2": "working set (all contour stores) larger than L2"},
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

@@ -11,6 +11,7 @@ _dp = ctypes.POINTER(ctypes.c_double)
 _vp = ctypes.c_void_p
 _sz = ctypes.c_size_t
 _szp = ctypes.POINTER(ctypes.c_size_t)
+_ip = ctypes.POINTER(ctypes.c_int)
 
 SCFT_OK = 0
 STATUS = {
@@ -71,6 +72,11 @@ SIGNATURES = {
     "scft_batch_iterate": (ctypes.c_int, [_vp, _sz, _dp, _dp]),
     "scft_batch_configure": (ctypes.c_int, [_vp, _sz, ctypes.c_int]),
     "scft_batch_autotune": (ctypes.c_int, [_vp, _sz, _szp, ctypes.POINTER(ctypes.c_int), _dp]),
+    "scft_batch_set_team_balance": (ctypes.c_int, [_vp, ctypes.c_double]),
+    "scft_batch_team_plan": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int), _szp, _szp, _dp, _dp]),
+    "scft_batch_launches_per_iteration": (ctypes.c_int, [_vp, _szp]),
+    "scft_team_schedule": (ctypes.c_int, [_sz, _ip, _ip, ctypes.c_int, ctypes.c_double, _ip, _sz, _ip, _ip, _ip,
+                                          _ip, _szp, _dp, _dp]),
     "scft_diblock_get_precision": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int)]),
     "scft_diblock_set_mixing": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double]),
     "scft_diblock_get_residuals": (ctypes.c_int, [_vp, _dp, _sz, _szp]),

@@ -13,7 +13,8 @@ from ._lib import check
 
 __all__ = ["BatchSCFT", "batch_config", "FORMS"]
 
-FORMS = {0: "automatic", 1: "alternating layout", 2: "two-phase", 3: "per-axis kernels"}
+FORMS = {0: "automatic", 1: "alternating layout", 2: "two-phase", 3: "per-axis kernels",
+         4: "one persistent launch (team kernel)"}
 
 
 def batch_config(n: int = 64, seed: int = 20261203, sizes=(16, 24, 32, 48, 64)):
@@ -108,18 +109,41 @@ class BatchSCFT:
         return {"F": F, "maxinc": mi}
 
     def launches_per_iteration(self) -> int:
-        """Kernel launches one batch iteration issues (summed over the instances' plans)."""
-        total = 0
-        for i in range(self.n):
-            d = ctypes.c_void_p()
-            check(_lib.load().scft_batch_instance(self._h, i, ctypes.byref(d)))
-            k = ctypes.c_size_t()
-            check(_lib.load().scft_diblock_launches_per_iteration(d, ctypes.byref(k)))
-            total += k.value
-        return total
+        """Kernel launches one batch iteration issues in the current configuration."""
+        k = ctypes.c_size_t()
+        check(_lib.load().scft_batch_launches_per_iteration(self._h, ctypes.byref(k)))
+        return k.value
+
+    def configure(self, nstreams: int = 8, form: int = 4):
+        """Worker streams and contour form (FORMS); 4 runs every instance's contour in one
+        persistent launch."""
+        check(_lib.load().scft_batch_configure(self._h, int(nstreams), int(form)))
+
+    def set_team_balance(self, balance: float):
+        """Form 4: how long a chain may run against the mean load of a CTA before its team grows."""
+        check(_lib.load().scft_batch_set_team_balance(self._h, float(balance)))
+
+    def team_plan(self) -> dict:
+        """The form-4 plan: CTAs, team tasks, instances in the launch, planned makespan and
+        its lower bound (us per iteration, cost model)."""
+        g, t, k = ctypes.c_int(), ctypes.c_size_t(), ctypes.c_size_t()
+        pl, lb = ctypes.c_double(), ctypes.c_double()
+        check(_lib.load().scft_batch_team_plan(self._h, ctypes.byref(g), ctypes.byref(t), ctypes.byref(k),
+                                               ctypes.byref(pl), ctypes.byref(lb)))
+        return {"grid": g.value, "tasks": t.value, "instances": k.value, "planned_us": pl.value,
+                "bound_us": lb.value}
 
     def configure(self, nstreams: int, form: int = 0):
         check(_lib.load().scft_batch_configure(self._h, int(nstreams), int(form)))
+
+    def set_wait_limit(self, spins: int | None = None):
+        """Poll limit of every bounded device wait of every instance (None: the default);
+        the one-launch form uses the smallest limit of its instances."""
+        L = _lib.load()
+        for i in range(self.n):
+            d = ctypes.c_void_p()
+            check(L.scft_batch_instance(self._h, i, ctypes.byref(d)))
+            check(L.scft_diblock_set_wait_limit(d, int(spins) if spins is not None else 20000000))
 
     def autotune(self, n_trial: int = 3):
         ns, form, ms = ctypes.c_size_t(), ctypes.c_int(), ctypes.c_double()

@@ -8,6 +8,7 @@
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -22,6 +23,7 @@
 #include "axis_fft.cuh"
 #include "axis_kernels.cuh"
 #include "contour_kernel.cuh"
+#include "contour_batch.cuh"
 #include "contour_cluster_f32.cuh"
 #include "contour_kernel_f32.cuh"
 #include "field_kernels.cuh"
@@ -1280,36 +1282,48 @@ struct scft_diblock_s {
         return SCFT_OK;
     }
 
+    // Parts of one iteration (bit mask): the batch kernel runs the contours of many
+    // instances in one launch between the instances' prep and field parts.
+    static constexpr int kPartPrep = 1, kPartContour = 2, kPartFields = 4, kPartAll = 7;
+
     template <typename T>
-    int enqueue_iteration(cudaStream_t st, T* wAds, T* wBds, T* q, T* qc, T** t) {
+    int enqueue_iteration(cudaStream_t st, T* wAds, T* wBds, T* q, T* qc, T** t, int parts = kPartAll) {
         const long long MM = (long long)M;
         const int blocks = grid_blocks(MM, 256);
         size_t launches = 0;
-        prep_kernel<T><<<blocks, 256, 0, st>>>(wA.p, wB.p, ksi.p, wAds, wBds, q, qc + U * M, xN, ds, MM);
-        CK(cudaGetLastError());
-        ++launches;
-        if (phase_events) CK(cudaEventRecord(phase_events[1], st));
-        const size_t before = solver->launches;
-        if (persistent) {
-            if constexpr (sizeof(T) == 8) CKR(launch_contour(st, wAds, wBds, q, qc));
-            else CKR(launch_contour_f32(st, wAds, wBds, q, qc));
-            ++solver->launches;
+        if (parts & kPartPrep) {
+            prep_kernel<T><<<blocks, 256, 0, st>>>(wA.p, wB.p, ksi.p, wAds, wBds, q, qc + U * M, xN, ds, MM);
+            CK(cudaGetLastError());
+            ++launches;
         }
-        for (size_t t_ = 0; t_ < U && !persistent; ++t_) {
-            // forward chain: q[t] -> q[t+1] with block A (t < NsA) or B
-            // backward chain: qc[U-t] -> qc[U-t-1] with the block of segment U-t-1
-            const T* w1 = t_ < NsA ? wAds : wBds;
-            const size_t ub = U - t_ - 1;
-            const T* w2 = ub < NsA ? wAds : wBds;
-            ChainIO<T> io[2];
-            io[0] = ChainIO<T>{q + t_ * M, q + (t_ + 1) * M, w1, w1};
-            io[1] = ChainIO<T>{qc + (ub + 1) * M, qc + ub * M, w2, w2};
-            T* t1[2] = {t[0], t[1]};
-            T* t2[2] = {t[2], t[3]};
-            CKR(solver->triplet<T>(2, io, t1, t2, st));
+        if (parts & kPartContour) {
+            if (phase_events) CK(cudaEventRecord(phase_events[1], st));
+            const size_t before = solver->launches;
+            if (persistent) {
+                if constexpr (sizeof(T) == 8) CKR(launch_contour(st, wAds, wBds, q, qc));
+                else CKR(launch_contour_f32(st, wAds, wBds, q, qc));
+                ++solver->launches;
+            }
+            for (size_t t_ = 0; t_ < U && !persistent; ++t_) {
+                // forward chain: q[t] -> q[t+1] with block A (t < NsA) or B
+                // backward chain: qc[U-t] -> qc[U-t-1] with the block of segment U-t-1
+                const T* w1 = t_ < NsA ? wAds : wBds;
+                const size_t ub = U - t_ - 1;
+                const T* w2 = ub < NsA ? wAds : wBds;
+                ChainIO<T> io[2];
+                io[0] = ChainIO<T>{q + t_ * M, q + (t_ + 1) * M, w1, w1};
+                io[1] = ChainIO<T>{qc + (ub + 1) * M, qc + ub * M, w2, w2};
+                T* t1[2] = {t[0], t[1]};
+                T* t2[2] = {t[2], t[3]};
+                CKR(solver->triplet<T>(2, io, t1, t2, st));
+            }
+            launches += solver->launches - before;
+            if (phase_events) CK(cudaEventRecord(phase_events[2], st));
         }
-        launches += solver->launches - before;
-        if (phase_events) CK(cudaEventRecord(phase_events[2], st));
+        if (!(parts & kPartFields)) {
+            launches_per_iter = launches;
+            return SCFT_OK;
+        }
         const int rblocks = (int)std::min<long long>(kRedMaxBlocks, (MM + kRedThreads - 1) / kRedThreads);
         q_reduce_kernel<T><<<rblocks, kRedThreads, 0, st>>>(qc, MM, partials.p, state.p);
         CK(cudaGetLastError());
@@ -1343,13 +1357,13 @@ struct scft_diblock_s {
         return SCFT_OK;
     }
 
-    int enqueue(cudaStream_t st) {
+    int enqueue(cudaStream_t st, int parts = kPartAll) {
         if (precision == SCFT_FP64) {
             double* t[4] = {d_t[0].p, d_t[1].p, d_t[2].p, d_t[3].p};
-            return enqueue_iteration<double>(st, d_wAds.p, d_wBds.p, d_q.p, d_qc.p, t);
+            return enqueue_iteration<double>(st, d_wAds.p, d_wBds.p, d_q.p, d_qc.p, t, parts);
         }
         float* t[4] = {f_t[0].p, f_t[1].p, f_t[2].p, f_t[3].p};
-        return enqueue_iteration<float>(st, f_wAds.p, f_wBds.p, f_q.p, f_qc.p, t);
+        return enqueue_iteration<float>(st, f_wAds.p, f_wBds.p, f_q.p, f_qc.p, t, parts);
     }
 
     int ensure_graph() {
@@ -2157,6 +2171,95 @@ int scft_diblock_time_phases(scft_diblock_t d, size_t n_iter, double out[4]) {
 // worker streams, into a single CUDA graph, so the instances' contour kernels run
 // concurrently on the SMs.  The autotuner picks the number of worker streams and the
 // contour-kernel form per batch by timing.
+// ---------------------------------------------------------------------------
+// Planner of the batch kernel (contour_batch.cuh): team sizes and CTA task lists.
+// ---------------------------------------------------------------------------
+// Cost model of one chain on a team of T CTAs (us): per unit and phase a fixed part (tile
+// fetch, waits, barriers, epilogue) plus the axis products, which grow as n^3; per phase
+// one exchange latency.
+static double team_unit_us(int n) { return 0.6 + 1.62e-5 * (double)n * n * n; }
+static double team_task_us(int n, int U, int T) { return (U + 1) * ((n / T) * team_unit_us(n) + 2.5); }
+
+// Chains j (grid side n[j], U[j] steps) on G CTAs.  Team sizes: start with one CTA per
+// chain; while a chain lasts longer than `balance` x the mean load of a CTA, its team grows
+// to the next divisor of n (at most min(n, G)).  Placement: list scheduling, largest team
+// work first; a team takes the T CTAs that are free first and starts when the last of them
+// is.  Every CTA's tasks are ordered by (planned start, chain): two teams that share CTAs
+// meet them in the same order everywhere, so the earliest unfinished task always has all
+// its members at it and the launch cannot deadlock.  Output: size[j]; tasks grouped by CTA
+// (CTA b runs tasks[begin[b] .. begin[b+1])); the planned makespan and the lower bound
+// (team work / G), both in us under the cost model.
+static int team_schedule(const std::vector<int>& n, const std::vector<int>& U, int G, double balance,
+                         std::vector<int>& size, std::vector<TeamTask>& tasks, std::vector<int>& begin,
+                         double& planned, double& bound) {
+    const size_t J = n.size();
+    if (U.size() != J || G < 1 || !(balance > 0.0)) return fail(SCFT_ERR_INVALID_ARG, "team schedule: bad arguments");
+    for (size_t j = 0; j < J; ++j)
+        if (n[j] < 1 || U[j] < 1) return fail(SCFT_ERR_INVALID_ARG, "team schedule: bad chain");
+    size.assign(J, 1);
+    std::vector<double> dur(J);
+    for (size_t j = 0; j < J; ++j) dur[j] = team_task_us(n[j], U[j], 1);
+    auto next_size = [&](size_t j) {
+        for (int t = size[j] + 1; t <= std::min(n[j], G); ++t)
+            if (n[j] % t == 0) return t;
+        return size[j];
+    };
+    for (int round = 0; round < 4096; ++round) {
+        double work = 0.0;
+        for (size_t j = 0; j < J; ++j) work += size[j] * dur[j];
+        const double limit = balance * work / G;
+        bool changed = false;
+        for (size_t j = 0; j < J; ++j) {
+            if (dur[j] <= limit) continue;
+            const int t = next_size(j);
+            if (t != size[j]) {
+                size[j] = t;
+                dur[j] = team_task_us(n[j], U[j], t);
+                changed = true;
+            }
+        }
+        if (!changed) break;
+    }
+    std::vector<size_t> order(J);
+    for (size_t j = 0; j < J; ++j) order[j] = j;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](size_t x, size_t y) { return size[x] * dur[x] > size[y] * dur[y]; });
+    struct Placed {
+        double start;
+        int chain, cta, rank, size;
+    };
+    std::vector<Placed> placed;
+    std::vector<double> avail(G, 0.0);
+    std::vector<int> idx(G);
+    bound = 0.0;
+    for (size_t j : order) {
+        for (int b = 0; b < G; ++b) idx[b] = b;
+        std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return avail[x] < avail[y]; });
+        double start = 0.0;
+        for (int r = 0; r < size[j]; ++r) start = std::max(start, avail[idx[r]]);
+        for (int r = 0; r < size[j]; ++r) {
+            avail[idx[r]] = start + dur[j];
+            placed.push_back(Placed{start, (int)j, idx[r], r, size[j]});
+        }
+        bound += size[j] * dur[j];
+    }
+    std::stable_sort(placed.begin(), placed.end(), [](const Placed& x, const Placed& y) {
+        if (x.cta != y.cta) return x.cta < y.cta;
+        if (x.start != y.start) return x.start < y.start;
+        return x.chain < y.chain;
+    });
+    tasks.resize(placed.size());
+    begin.assign(G + 1, 0);
+    for (size_t t = 0; t < placed.size(); ++t) {
+        tasks[t] = TeamTask{placed[t].chain, placed[t].rank, placed[t].size, 0};
+        begin[placed[t].cta + 1]++;
+    }
+    for (int b = 0; b < G; ++b) begin[b + 1] += begin[b];
+    planned = J ? *std::max_element(avail.begin(), avail.end()) : 0.0;
+    bound /= G;
+    return SCFT_OK;
+}
+
 struct scft_batch_s {
     int device = 0;
     std::vector<scft_solver_t> solvers;
@@ -2169,6 +2272,136 @@ struct scft_batch_s {
     cudaGraphExec_t gexec = nullptr;
     size_t nstreams = 8;
     int form = 0;
+
+    // Form 4: the contours of every instance whose own plan is the alternating FP64 kernel
+    // run in ONE persistent launch of batch_contour_kernel (contour_batch.cuh); the
+    // instances' prep and field kernels stay on the worker streams before and after it.
+    double team_balance = 1.0;      // a chain's team grows until it lasts <= balance x the mean load
+    std::vector<char> in_team;      // per instance: its contour runs in the batch kernel
+    DevBuf<TeamChain> team_chains;
+    DevBuf<TeamTask> team_tasks;
+    DevBuf<int> team_begin;
+    DevBuf<unsigned> team_flags;    // every chain's exchange flags, zeroed before each launch
+    DevBuf<unsigned> team_abort;
+    int team_grid = 0;              // CTAs of the launch (0: no instance in the batch kernel)
+    size_t team_smem = 0;
+    size_t team_ntasks = 0;
+    double team_planned_us = 0.0;   // makespan of the plan under the cost model
+    double team_bound_us = 0.0;     // total team work / CTAs under the same model
+    size_t launches = 0;            // kernel launches of one batch iteration
+
+    // Team sizes, CTA assignment and device-side task lists of the batch kernel.
+    int plan_teams() {
+        const size_t n = runs.size();
+        in_team.assign(n, 0);
+        team_grid = 0;
+        struct Ch {
+            size_t run;
+            int c, n, U, form;
+        };
+        std::vector<Ch> chs;
+        size_t smem = 0;
+        for (size_t i = 0; i < n; ++i) {
+            scft_diblock_t d = runs[i];
+            if (d->precision != SCFT_FP64 || !d->persistent || !d->alternating || !d->d_q.p || !d->ctrl.p) continue;
+            const int side = (int)d->solver->grid_phy[0];
+            const int f = team_form_for(side, d->solver->ops->eo[0] != 0, d->alt_eo2);
+            if (f < 0) continue;
+            in_team[i] = 1;
+            smem = std::max(smem, team_form_smem(f));
+            for (int c = 0; c < 2; ++c) chs.push_back(Ch{i, c, side, (int)d->U, f});
+        }
+        if (chs.empty()) return SCFT_OK;
+        int sms = 0, dev_smem = 0;
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+        CK(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+        if (smem > (size_t)dev_smem) return fail(SCFT_ERR_UNSUPPORTED, "batch kernel: shared memory beyond the limit");
+        CK(cudaFuncSetAttribute(batch_contour_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int per_sm = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_contour_kernel, kContourThreads, smem));
+        if (per_sm < 1) return fail(SCFT_ERR_UNSUPPORTED, "batch kernel: no block fits on a multiprocessor");
+        const int G = per_sm * sms;
+
+        std::vector<int> side(chs.size()), steps(chs.size()), size(chs.size());
+        for (size_t j = 0; j < chs.size(); ++j) {
+            side[j] = chs[j].n;
+            steps[j] = chs[j].U;
+        }
+        std::vector<TeamTask> tasks;
+        std::vector<int> begin;
+        double planned = 0.0, bound = 0.0;
+        CKR(team_schedule(side, steps, G, team_balance, size, tasks, begin, planned, bound));
+
+        // chain descriptors (tensor maps of each instance's stores and Boltzmann factors)
+        size_t nflags = 0;
+        std::vector<size_t> flag_off(chs.size());
+        for (size_t j = 0; j < chs.size(); ++j) {
+            flag_off[j] = nflags;
+            nflags += 2 * (size_t)chs[j].n * chs[j].n;
+        }
+        CKR(team_flags.alloc(nflags));
+        if (!team_abort.p) CKR(team_abort.alloc(1));
+        std::vector<TeamChain> hc(chs.size());
+        for (size_t j = 0; j < chs.size(); ++j) {
+            const Ch& h = chs[j];
+            scft_diblock_t d = runs[h.run];
+            TeamChain& t = hc[j];
+            std::memset(&t, 0, sizeof(TeamChain));
+            double* q = h.c == 0 ? d->d_q.p : d->d_qc.p;
+            for (int v = 0; v < 2; ++v) {  // plane [0] and slab [1] views, as launch_contour
+                CKR(encode_panel_map(&t.tm_q[v], q, h.n, (long long)h.U + 1, v == 0));
+                CKR(encode_panel_map(&t.tm_w[0][v], d->d_wAds.p, h.n, 0, v == 0));
+                CKR(encode_panel_map(&t.tm_w[1][v], d->d_wBds.p, h.n, 0, v == 0));
+            }
+            t.q = q;
+            t.xbuf = d->d_xch.p + (size_t)h.c * 2 * d->M;
+            t.ops = d->alt_eo2 ? d->solver->ops->d_packed2.p : d->solver->ops->d_packed.p;
+            t.flags = team_flags.p + flag_off[j];
+            t.error = d->ctrl.p + 1;
+            t.slot0 = h.c == 0 ? 0 : (long long)h.U;
+            t.NsA = (long long)d->NsA;
+            t.dir = h.c == 0 ? 1 : -1;
+            t.U = h.U;
+            t.n = h.n;
+            t.form = h.form;
+        }
+        CKR(team_chains.alloc(hc.size()));
+        CKR(team_tasks.alloc(tasks.size()));
+        CKR(team_begin.alloc(begin.size()));
+        CK(cudaMemcpy(team_chains.p, hc.data(), hc.size() * sizeof(TeamChain), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(team_tasks.p, tasks.data(), tasks.size() * sizeof(TeamTask), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(team_begin.p, begin.data(), begin.size() * sizeof(int), cudaMemcpyHostToDevice));
+        team_grid = G;
+        team_smem = smem;
+        team_ntasks = tasks.size();
+        team_planned_us = planned;
+        team_bound_us = bound;
+        return SCFT_OK;
+    }
+
+    int launch_teams(cudaStream_t st) {
+        CK(cudaMemsetAsync(team_flags.p, 0, team_flags.n * sizeof(unsigned), st));
+        CK(cudaMemsetAsync(team_abort.p, 0, sizeof(unsigned), st));
+        BatchContourArgs a{};
+        a.chains = team_chains.p;
+        a.tasks = team_tasks.p;
+        a.task_begin = team_begin.p;
+        a.abort = team_abort.p;
+        a.spin_limit = runs[0]->spin_limit;  // the smallest wait limit of the instances
+        for (auto d : runs) a.spin_limit = std::min(a.spin_limit, d->spin_limit);
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3((unsigned)team_grid);
+        cfg.blockDim = dim3(kContourThreads);
+        cfg.dynamicSmemBytes = team_smem;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        CK(cudaLaunchKernelEx(&cfg, batch_contour_kernel, a));
+        return SCFT_OK;
+    }
 
     void drop_graph() {
         if (gexec) cudaGraphExecDestroy(gexec);
@@ -2206,22 +2439,49 @@ struct scft_batch_s {
 
     int build_graph() {
         drop_graph();
+        const int ff = form == 4 ? 0 : form;  // the instances' own plan under form 4: automatic
         for (auto d : runs) {
-            d->force_form = form;
-            if (d->captured_gen == d->solver->ops_gen && d->last_form != form) d->captured_gen = ~0ULL;
-            d->last_form = form;
+            d->force_form = ff;
+            if (d->captured_gen == d->solver->ops_gen && d->last_form != ff) d->captured_gen = ~0ULL;
+            d->last_form = ff;
             CKR(diblock_prepare(d, false));
         }
+        team_grid = 0;
+        in_team.assign(runs.size(), 0);
+        if (form == 4) CKR(plan_teams());
+        const bool teams = team_grid > 0;
+        using DB = scft_diblock_s;
         CK(cudaStreamBeginCapture(main, cudaStreamCaptureModeThreadLocal));
         int r = SCFT_OK;
+        launches = 0;
+        std::vector<size_t> pre(runs.size(), 0);
         cudaError_t e = cudaEventRecord(fork, main);
         for (size_t w = 0; w < nstreams && e == cudaSuccess; ++w) e = cudaStreamWaitEvent(streams[w], fork, 0);
-        for (size_t i = 0; i < runs.size() && r == SCFT_OK && e == cudaSuccess; ++i)
-            r = runs[i]->enqueue(streams[i % nstreams]);
+        for (size_t i = 0; i < runs.size() && r == SCFT_OK && e == cudaSuccess; ++i) {
+            r = runs[i]->enqueue(streams[i % nstreams], in_team[i] ? DB::kPartPrep : DB::kPartAll);
+            pre[i] = runs[i]->launches_per_iter;
+        }
         for (size_t w = 0; w < nstreams && e == cudaSuccess; ++w) {
             e = cudaEventRecord(joins[w], streams[w]);
             if (e == cudaSuccess) e = cudaStreamWaitEvent(main, joins[w], 0);
         }
+        if (teams && r == SCFT_OK && e == cudaSuccess) {
+            // one persistent launch: the contours of every instance in in_team
+            r = launch_teams(main);
+            ++launches;
+            if (r == SCFT_OK) e = cudaEventRecord(fork, main);
+            for (size_t w = 0; w < nstreams && e == cudaSuccess; ++w) e = cudaStreamWaitEvent(streams[w], fork, 0);
+            for (size_t i = 0; i < runs.size() && r == SCFT_OK && e == cudaSuccess; ++i) {
+                if (!in_team[i]) continue;
+                r = runs[i]->enqueue(streams[i % nstreams], DB::kPartFields);
+                runs[i]->launches_per_iter += pre[i];  // the instance's own kernels; the contour is counted once above
+            }
+            for (size_t w = 0; w < nstreams && e == cudaSuccess; ++w) {
+                e = cudaEventRecord(joins[w], streams[w]);
+                if (e == cudaSuccess) e = cudaStreamWaitEvent(main, joins[w], 0);
+            }
+        }
+        for (auto d : runs) launches += d->launches_per_iter;
         cudaGraph_t g = nullptr;
         const cudaError_t e2 = cudaStreamEndCapture(main, &g);
         if (r != SCFT_OK) {
@@ -2239,7 +2499,10 @@ struct scft_batch_s {
 
     // n_iter iterations; per-iteration F and max incompressibility of every instance
     int run(size_t n_iter, double* F, double* maxinc) {
-        if (!gexec) CKR(build_graph());
+        // rebuild when an instance's plan went stale (new operators, a new wait limit)
+        bool stale = !gexec;
+        for (auto d : runs) stale = stale || d->captured_gen != d->solver->ops_gen;
+        if (stale) CKR(build_graph());
         const size_t n = runs.size();
         size_t done = 0;
         std::vector<double> h;
@@ -2248,6 +2511,16 @@ struct scft_batch_s {
             IterState zero{};
             for (auto d : runs) CK(cudaMemcpyAsync(d->state.p, &zero, sizeof(IterState), cudaMemcpyHostToDevice, main));
             for (size_t k = 0; k < chunk; ++k) CK(cudaGraphLaunch(gexec, main));
+            // device-side errors first (a kernel that gave up leaves unfinished fields, which
+            // are not a numeric failure), every instance's word read and cleared
+            {
+                int first = SCFT_OK;
+                for (size_t i = 0; i < n; ++i) {
+                    const int r = diblock_check_device_error(runs[i], main);
+                    if (first == SCFT_OK) first = r;
+                }
+                if (first != SCFT_OK) return first;
+            }
             for (size_t i = 0; i < n; ++i) {
                 scft_diblock_t d = runs[i];
                 h.resize(chunk * HIST_STRIDE);
@@ -2259,7 +2532,6 @@ struct scft_batch_s {
                     if (maxinc) maxinc[(done + k) * n + i] = rr[HIST_MAXINC];
                     if (rr[HIST_FLAGS] != 0.0) return fail(SCFT_ERR_NUMERIC, "instance " + std::to_string(i) + ": Q <= 0 or NaN");
                 }
-                CKR(diblock_check_device_error(d, main));
                 d->last_iter_precision = d->precision;
             }
             done += chunk;
@@ -2332,7 +2604,7 @@ int scft_batch_iterate(scft_batch_t b, size_t n_iter, double* F, double* maxinc)
 }
 
 int scft_batch_configure(scft_batch_t b, size_t nstreams, int form) {
-    if (!b || form < 0 || form > 3) return fail(SCFT_ERR_INVALID_ARG, "bad configuration");
+    if (!b || form < 0 || form > 4) return fail(SCFT_ERR_INVALID_ARG, "bad configuration");
     CK(cudaSetDevice(b->device));
     CK(cudaStreamSynchronize(b->main));
     b->drop_graph();
@@ -2352,17 +2624,22 @@ int scft_batch_autotune(scft_batch_t b, size_t n_trial, size_t* best_nstreams, i
         std::vector<std::vector<double>> keepA, keepB;
         size_t ns0;
         int form0;
+        double balance0;
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         bool keep_config = false;
         ~Guard() {
             if (e0) cudaEventDestroy(e0);
             if (e1) cudaEventDestroy(e1);
             cudaStreamSynchronize(b->main);
-            if (!keep_config) scft_batch_configure(b, ns0, form0);
+            if (!keep_config) {
+                scft_batch_configure(b, ns0, form0);
+                b->team_balance = balance0;
+            }
             for (size_t i = 0; i < keepA.size(); ++i)
                 if (!keepA[i].empty()) scft_diblock_set_fields(b->runs[i], keepA[i].data(), keepB[i].data());
         }
-    } g{b, std::vector<std::vector<double>>(n), std::vector<std::vector<double>>(n), b->nstreams, b->form};
+    } g{b, std::vector<std::vector<double>>(n), std::vector<std::vector<double>>(n), b->nstreams, b->form,
+        b->team_balance};
     for (size_t i = 0; i < n; ++i) {
         std::vector<double> a(b->runs[i]->M), bb(b->runs[i]->M);
         CKR(scft_diblock_get_fields(b->runs[i], nullptr, nullptr, a.data(), bb.data()));
@@ -2374,31 +2651,104 @@ int scft_batch_autotune(scft_batch_t b, size_t n_trial, size_t* best_nstreams, i
     double best = 1e300;
     size_t bs = b->nstreams;
     int bf = b->form;
+    double bb = b->team_balance;
     const size_t cand_streams[] = {2, 4, 8, 16, 32};
-    const int cand_forms[] = {0, 2};
+    const int cand_forms[] = {0, 2, 4};
+    // form 4: the team-size balance (how long a chain may run against the mean load of a CTA)
+    const double cand_balance[] = {0.5, 1.0, 2.0};
+    auto trial = [&](size_t ns, int f, double balance) -> int {
+        CKR(scft_batch_configure(b, ns, f));
+        b->team_balance = balance;
+        CKR(b->run(1, nullptr, nullptr));  // capture + warm up
+        CK(cudaEventRecord(g.e0, b->main));
+        CKR(b->run(n_trial, nullptr, nullptr));
+        CK(cudaEventRecord(g.e1, b->main));
+        CK(cudaEventSynchronize(g.e1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, g.e0, g.e1));
+        if (ms < best) {
+            best = ms;
+            bs = ns;
+            bf = f;
+            bb = balance;
+        }
+        return SCFT_OK;
+    };
     for (int f : cand_forms) {
         for (size_t ns : cand_streams) {
             if (ns > n && ns != cand_streams[0]) continue;
-            CKR(scft_batch_configure(b, ns, f));
-            CKR(b->run(1, nullptr, nullptr));  // capture + warm up
-            CK(cudaEventRecord(g.e0, b->main));
-            CKR(b->run(n_trial, nullptr, nullptr));
-            CK(cudaEventRecord(g.e1, b->main));
-            CK(cudaEventSynchronize(g.e1));
-            float ms = 0.f;
-            CK(cudaEventElapsedTime(&ms, g.e0, g.e1));
-            if (ms < best) {
-                best = ms;
-                bs = ns;
-                bf = f;
+            if (f == 4) {
+                // the worker streams only carry the small per-instance kernels here
+                if (ns != 4 && ns != 16) continue;
+                for (double bal : cand_balance) CKR(trial(ns, f, bal));
+            } else {
+                CKR(trial(ns, f, b->team_balance));
             }
         }
     }
     CKR(scft_batch_configure(b, bs, bf));
+    b->team_balance = bb;
     g.keep_config = true;  // the guard now only restores the fields and frees the events
     if (best_nstreams) *best_nstreams = bs;
     if (best_form) *best_form = bf;
     if (best_ms) *best_ms = best / (double)n_trial;
+    return SCFT_OK;
+}
+
+int scft_team_schedule(size_t nchains, const int* n, const int* U, int G, double balance, int* size, size_t cap,
+                       int* task_chain, int* task_rank, int* task_size, int* task_begin, size_t* ntasks,
+                       double* planned_us, double* bound_us) {
+    if (!n || !U || !size || !task_begin || !ntasks) return fail(SCFT_ERR_INVALID_ARG, "null argument");
+    std::vector<int> vn(n, n + nchains), vu(U, U + nchains), sz;
+    std::vector<TeamTask> tasks;
+    std::vector<int> begin;
+    double planned = 0.0, bound = 0.0;
+    CKR(team_schedule(vn, vu, G, balance, sz, tasks, begin, planned, bound));
+    *ntasks = tasks.size();
+    if (tasks.size() > cap || ((!task_chain || !task_rank || !task_size) && !tasks.empty()))
+        return fail(SCFT_ERR_INVALID_ARG, "team schedule: task arrays too small (" + std::to_string(tasks.size()) +
+                                              " tasks)");
+    for (size_t j = 0; j < nchains; ++j) size[j] = sz[j];
+    for (size_t t = 0; t < tasks.size(); ++t) {
+        task_chain[t] = tasks[t].chain;
+        task_rank[t] = tasks[t].rank;
+        task_size[t] = tasks[t].size;
+    }
+    for (int b = 0; b <= G; ++b) task_begin[b] = begin[b];
+    if (planned_us) *planned_us = planned;
+    if (bound_us) *bound_us = bound;
+    return SCFT_OK;
+}
+
+int scft_batch_set_team_balance(scft_batch_t b, double balance) {
+    if (!b || !(balance > 0.0)) return fail(SCFT_ERR_INVALID_ARG, "bad argument");
+    CK(cudaSetDevice(b->device));
+    CK(cudaStreamSynchronize(b->main));
+    b->drop_graph();
+    b->team_balance = balance;
+    return SCFT_OK;
+}
+
+int scft_batch_team_plan(scft_batch_t b, int* grid, size_t* ntasks, size_t* ninstances, double* planned_us,
+                         double* bound_us) {
+    if (!b) return fail(SCFT_ERR_INVALID_ARG, "null handle");
+    CK(cudaSetDevice(b->device));
+    if (!b->gexec) CKR(b->build_graph());
+    size_t k = 0;
+    for (char c : b->in_team) k += c ? 1 : 0;
+    if (grid) *grid = b->team_grid;
+    if (ntasks) *ntasks = b->team_grid ? b->team_ntasks : 0;
+    if (ninstances) *ninstances = k;
+    if (planned_us) *planned_us = b->team_grid ? b->team_planned_us : 0.0;
+    if (bound_us) *bound_us = b->team_grid ? b->team_bound_us : 0.0;
+    return SCFT_OK;
+}
+
+int scft_batch_launches_per_iteration(scft_batch_t b, size_t* out) {
+    if (!b || !out) return fail(SCFT_ERR_INVALID_ARG, "null argument");
+    CK(cudaSetDevice(b->device));
+    if (!b->gexec) CKR(b->build_graph());
+    *out = b->launches;
     return SCFT_OK;
 }
 

@@ -4,7 +4,7 @@ the same results; the autotuner restores the fields it advanced."""
 import numpy as np
 import pytest
 
-from crysscft_sample_b200 import batch, fields, scft, solvers
+from crysscft_sample_b200 import _lib, batch, fields, scft, solvers
 from oracle import ref
 
 pytestmark = pytest.mark.gpu
@@ -72,6 +72,66 @@ def test_every_kernel_form_agrees(gpu, form):
     assert np.allclose(h["F"], h0["F"], rtol=1e-11, atol=0)
 
 
+def _mixed(n=10, seed=11):
+    # every configured grid side (reduced 16, 24, 32, 48, 64) at least once
+    cfg = batch.batch_config(n, seed=seed)
+    for i, side in enumerate((16, 24, 32, 48, 64)):
+        cfg[i]["N"] = (2 * side,) * 3
+    return cfg
+
+
+@pytest.mark.parametrize("balance", [0.25, 1.0, 4.0])
+def test_one_launch_form_is_bit_identical_to_per_instance_kernels(gpu, balance):
+    # form 4 runs each chain on a team of CTAs that own several planes / slabs each; every
+    # unit does the per-instance kernel's arithmetic in the same order, so the results are
+    # the same bits whatever the team sizes (balance 4: one CTA per chain at every size)
+    inst = _mixed()
+    B1 = batch.BatchSCFT("PMMM", inst)
+    B1.configure(4, 1)
+    B1.seed_fields()
+    h1 = B1.iterate(3)
+    B4 = batch.BatchSCFT("PMMM", inst)
+    B4.configure(4, 4)
+    B4.set_team_balance(balance)
+    B4.seed_fields()
+    plan = B4.team_plan()
+    assert plan["instances"] == len(inst) and plan["grid"] > 0
+    assert B4.launches_per_iteration() < B1.launches_per_iteration()
+    h4 = B4.iterate(3)
+    assert np.array_equal(h4["F"], h1["F"])
+    assert np.array_equal(h4["maxinc"], h1["maxinc"])
+    for i in range(len(inst)):
+        f1, f4 = B1.get_fields(i), B4.get_fields(i)
+        for k in f1:
+            assert np.array_equal(f4[k], f1[k]), f"instance {i} {k}"
+    B1.close()
+    B4.close()
+
+
+def test_one_launch_form_timeout_is_reported_and_the_batch_survives(gpu):
+    # a poll limit of 1: the first flag or tile-load wait of the batch kernel runs out; the
+    # CTA sets the abort word, drains its own copies and leaves, the others stop waiting
+    inst = _mixed(6, seed=3)
+    ref_b = batch.BatchSCFT("PMMM", inst)
+    ref_b.configure(4, 4)
+    ref_b.seed_fields()
+    want = ref_b.iterate(2)["F"]
+    B = batch.BatchSCFT("PMMM", inst)
+    B.configure(4, 4)
+    B.seed_fields()
+    B.iterate(1)
+    B.set_wait_limit(1)
+    with pytest.raises(_lib.ScftError) as e:
+        B.iterate(1)
+    assert e.value.status == 7  # SCFT_ERR_TIMEOUT
+    B.set_wait_limit()
+    B.seed_fields()
+    got = B.iterate(2)["F"]
+    assert np.array_equal(got, want)
+    B.close()
+    ref_b.close()
+
+
 def test_autotune_restores_fields(gpu):
     inst = _instances()
     B = batch.BatchSCFT("PMMM", inst)
@@ -93,7 +153,9 @@ def test_batching_configuration_200_iterations(gpu):
     cfg = batch.batch_config(64)
     B = batch.BatchSCFT("PMMM", cfg, ds=0.01)
     B.seed_fields()
-    B.autotune(2)
+    tuned = B.autotune(2)
+    B.configure(tuned["nstreams"], 4)  # the single persistent launch, whatever the autotuner chose
+    assert B.team_plan()["instances"] == len(cfg)
     hb = B.iterate(200)
     assert np.all(np.isfinite(hb["F"]))
     for i, it in enumerate(cfg):
