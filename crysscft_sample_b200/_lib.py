@@ -72,10 +72,10 @@ SIGNATURES = {
     "scft_batch_iterate": (ctypes.c_int, [_vp, _sz, _dp, _dp]),
     "scft_batch_configure": (ctypes.c_int, [_vp, _sz, ctypes.c_int]),
     "scft_batch_autotune": (ctypes.c_int, [_vp, _sz, _szp, ctypes.POINTER(ctypes.c_int), _dp]),
-    "scft_batch_set_team_balance": (ctypes.c_int, [_vp, ctypes.c_double]),
+    "scft_batch_set_team_sizes": (ctypes.c_int, [_vp, _sz, _ip, _ip]),
     "scft_batch_team_plan": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int), _szp, _szp, _dp, _dp]),
     "scft_batch_launches_per_iteration": (ctypes.c_int, [_vp, _szp]),
-    "scft_team_schedule": (ctypes.c_int, [_sz, _ip, _ip, ctypes.c_int, ctypes.c_double, _ip, _sz, _ip, _ip, _ip,
+    "scft_team_schedule": (ctypes.c_int, [_sz, _ip, _ip, ctypes.c_int, _sz, _ip, _ip, _ip, _sz, _ip, _ip, _ip,
                                           _ip, _szp, _dp, _dp]),
     "scft_diblock_get_precision": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int)]),
     "scft_diblock_set_mixing": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double]),

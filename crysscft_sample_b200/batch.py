@@ -119,9 +119,11 @@ class BatchSCFT:
         persistent launch."""
         check(_lib.load().scft_batch_configure(self._h, int(nstreams), int(form)))
 
-    def set_team_balance(self, balance: float):
-        """Form 4: how long a chain may run against the mean load of a CTA before its team grows."""
-        check(_lib.load().scft_batch_set_team_balance(self._h, float(balance)))
+    def set_team_sizes(self, sizes: dict):
+        """Form 4: fixed team sizes {grid side: CTAs per chain}; other sides get the planner's choice."""
+        sides = (ctypes.c_int * max(1, len(sizes)))(*[int(k) for k in sizes])
+        vals = (ctypes.c_int * max(1, len(sizes)))(*[int(v) for v in sizes.values()])
+        check(_lib.load().scft_batch_set_team_sizes(self._h, len(sizes), sides, vals))
 
     def team_plan(self) -> dict:
         """The form-4 plan: CTAs, team tasks, instances in the launch, planned makespan and

@@ -2174,74 +2174,139 @@ int scft_diblock_time_phases(scft_diblock_t d, size_t n_iter, double out[4]) {
 // ---------------------------------------------------------------------------
 // Planner of the batch kernel (contour_batch.cuh): team sizes and CTA task lists.
 // ---------------------------------------------------------------------------
-// Cost model of one chain on a team of T CTAs (us): per unit and phase a fixed part (tile
-// fetch, waits, barriers, epilogue) plus the axis products, which grow as n^3; per phase
-// one exchange latency.
-static double team_unit_us(int n) { return 0.6 + 1.62e-5 * (double)n * n * n; }
-static double team_task_us(int n, int U, int T) { return (U + 1) * ((n / T) * team_unit_us(n) + 2.5); }
+// Cost model of one chain on a team of T CTAs (us), fitted to the batch kernel on a B200
+// with every SM busy: per unit and phase 1.9 us of fixed work (tile fetch, waits, barriers,
+// epilogue, stores) plus the axis products, ~1.02e-3 n^2 us; per phase one exchange
+// (release, flag round trip) of ~2.3 us.
+static double team_unit_us(int n) { return 1.9 + 1.02e-3 * (double)n * n; }
+static double team_task_us(int n, int U, int T) { return (U + 1) * ((n / T) * team_unit_us(n) + 2.3); }
 
-// Chains j (grid side n[j], U[j] steps) on G CTAs.  Team sizes: start with one CTA per
-// chain; while a chain lasts longer than `balance` x the mean load of a CTA, its team grows
-// to the next divisor of n (at most min(n, G)).  Placement: list scheduling, largest team
-// work first; a team takes the T CTAs that are free first and starts when the last of them
-// is.  Every CTA's tasks are ordered by (planned start, chain): two teams that share CTAs
-// meet them in the same order everywhere, so the earliest unfinished task always has all
-// its members at it and the launch cannot deadlock.  Output: size[j]; tasks grouped by CTA
-// (CTA b runs tasks[begin[b] .. begin[b+1])); the planned makespan and the lower bound
-// (team work / G), both in us under the cost model.
-static int team_schedule(const std::vector<int>& n, const std::vector<int>& U, int G, double balance,
-                         std::vector<int>& size, std::vector<TeamTask>& tasks, std::vector<int>& begin,
-                         double& planned, double& bound) {
+// First-fit decreasing of durations d into columns of capacity D: the column loads, or
+// an empty vector if one duration exceeds D.  col[i] receives the column of item i.
+static std::vector<double> pack_columns(const std::vector<double>& d, double D, std::vector<int>& col) {
+    std::vector<size_t> order(d.size());
+    for (size_t i = 0; i < d.size(); ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return d[x] > d[y]; });
+    std::vector<double> load;
+    col.assign(d.size(), -1);
+    for (size_t i : order) {
+        if (d[i] > D) return {};
+        size_t c = 0;
+        while (c < load.size() && load[c] + d[i] > D) ++c;
+        if (c == load.size()) load.push_back(0.0);
+        load[c] += d[i];
+        col[i] = (int)c;
+    }
+    return load;
+}
+
+// Chains j (grid side n[j], U[j] steps) on G CTAs.  Chains of one grid side form a class;
+// for a target makespan D a class with team size T runs in columns of T CTAs, its chains
+// stacked in the columns by first-fit decreasing, and costs T x columns CTAs; every class
+// takes the team size (a divisor of n, or the caller's fixed size) that costs fewest CTAs,
+// and D is the smallest target (bisection) whose classes fit in G CTAs.  Every CTA belongs
+// to one column and runs that column's chains in order, all CTAs of a column the same
+// sequence, so no team ever waits for a CTA busy elsewhere.  Output: size[j]; tasks grouped
+// by CTA (CTA b runs tasks[begin[b] .. begin[b+1]) in order); the planned makespan and the
+// lower bound (team work / G), in us per iteration under the cost model.
+static int team_schedule(const std::vector<int>& n, const std::vector<int>& U, int G,
+                         const std::map<int, int>& fixed, std::vector<int>& size, std::vector<TeamTask>& tasks,
+                         std::vector<int>& begin, double& planned, double& bound) {
     const size_t J = n.size();
-    if (U.size() != J || G < 1 || !(balance > 0.0)) return fail(SCFT_ERR_INVALID_ARG, "team schedule: bad arguments");
+    if (U.size() != J || G < 1) return fail(SCFT_ERR_INVALID_ARG, "team schedule: bad arguments");
     for (size_t j = 0; j < J; ++j)
         if (n[j] < 1 || U[j] < 1) return fail(SCFT_ERR_INVALID_ARG, "team schedule: bad chain");
-    size.assign(J, 1);
-    std::vector<double> dur(J);
-    for (size_t j = 0; j < J; ++j) dur[j] = team_task_us(n[j], U[j], 1);
-    auto next_size = [&](size_t j) {
-        for (int t = size[j] + 1; t <= std::min(n[j], G); ++t)
-            if (n[j] % t == 0) return t;
-        return size[j];
-    };
-    for (int round = 0; round < 4096; ++round) {
-        double work = 0.0;
-        for (size_t j = 0; j < J; ++j) work += size[j] * dur[j];
-        const double limit = balance * work / G;
-        bool changed = false;
-        for (size_t j = 0; j < J; ++j) {
-            if (dur[j] <= limit) continue;
-            const int t = next_size(j);
-            if (t != size[j]) {
-                size[j] = t;
-                dur[j] = team_task_us(n[j], U[j], t);
-                changed = true;
-            }
+    std::map<int, std::vector<size_t>> classes;
+    for (size_t j = 0; j < J; ++j) classes[n[j]].push_back(j);
+    std::map<int, std::vector<int>> cand;  // team sizes a class may take
+    for (const auto& c : classes) {
+        auto it = fixed.find(c.first);
+        if (it != fixed.end()) {
+            if (it->second < 1 || c.first % it->second || it->second > G)
+                return fail(SCFT_ERR_INVALID_ARG, "team schedule: a fixed team size must divide the grid side and fit");
+            cand[c.first] = {it->second};
+        } else {
+            for (int t = 1; t <= std::min(c.first, G); ++t)
+                if (c.first % t == 0) cand[c.first].push_back(t);
         }
-        if (!changed) break;
     }
-    std::vector<size_t> order(J);
-    for (size_t j = 0; j < J; ++j) order[j] = j;
-    std::stable_sort(order.begin(), order.end(),
-                     [&](size_t x, size_t y) { return size[x] * dur[x] > size[y] * dur[y]; });
+    struct Choice {
+        int T = 0;
+        std::vector<double> load;
+        std::vector<int> col;
+    };
+    // the cheapest choice of every class for target D; false if they need more than G CTAs
+    auto plan_for = [&](double D, std::map<int, Choice>& out) {
+        long long total = 0;
+        for (const auto& c : classes) {
+            Choice best;
+            long long best_cost = -1;
+            for (int T : cand[c.first]) {
+                std::vector<double> d(c.second.size());
+                for (size_t i = 0; i < d.size(); ++i) d[i] = team_task_us(c.first, U[c.second[i]], T);
+                Choice ch;
+                ch.T = T;
+                ch.load = pack_columns(d, D, ch.col);
+                if (ch.load.empty()) continue;
+                const long long cost = (long long)T * ch.load.size();
+                if (best_cost < 0 || cost < best_cost) {
+                    best_cost = cost;
+                    best = std::move(ch);
+                }
+            }
+            if (best_cost < 0) return false;
+            total += best_cost;
+            out[c.first] = std::move(best);
+        }
+        return total <= G;
+    };
+    double hi = 0.0;
+    for (size_t j = 0; j < J; ++j) hi += team_task_us(n[j], U[j], 1);
+    std::map<int, Choice> plan;
+    if (!plan_for(hi, plan)) {
+        // more classes than CTAs: only then does one column per class not fit
+        return fail(SCFT_ERR_UNSUPPORTED, "team schedule: more grid sizes than CTAs");
+    }
+    double lo = 0.0;
+    for (int it = 0; it < 60; ++it) {
+        const double mid = 0.5 * (lo + hi);
+        std::map<int, Choice> p;
+        if (plan_for(mid, p)) {
+            hi = mid;
+            plan = std::move(p);
+        } else {
+            lo = mid;
+        }
+    }
+    // place the columns on consecutive CTAs; chains of a column run in FFD order
+    size.assign(J, 1);
     struct Placed {
         double start;
         int chain, cta, rank, size;
     };
     std::vector<Placed> placed;
-    std::vector<double> avail(G, 0.0);
-    std::vector<int> idx(G);
+    int base = 0;
+    planned = 0.0;
     bound = 0.0;
-    for (size_t j : order) {
-        for (int b = 0; b < G; ++b) idx[b] = b;
-        std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return avail[x] < avail[y]; });
-        double start = 0.0;
-        for (int r = 0; r < size[j]; ++r) start = std::max(start, avail[idx[r]]);
-        for (int r = 0; r < size[j]; ++r) {
-            avail[idx[r]] = start + dur[j];
-            placed.push_back(Placed{start, (int)j, idx[r], r, size[j]});
+    for (const auto& c : classes) {
+        const Choice& ch = plan[c.first];
+        std::vector<double> t0(ch.load.size(), 0.0);
+        std::vector<size_t> order(c.second.size());
+        for (size_t i = 0; i < order.size(); ++i) order[i] = i;
+        std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) {
+            return U[c.second[x]] > U[c.second[y]];  // FFD order: longest first within a column
+        });
+        for (size_t i : order) {
+            const size_t j = c.second[i];
+            const int col = ch.col[i];
+            const double d = team_task_us(n[j], U[j], ch.T);
+            size[j] = ch.T;
+            for (int r = 0; r < ch.T; ++r) placed.push_back(Placed{t0[col], (int)j, base + col * ch.T + r, r, ch.T});
+            t0[col] += d;
+            bound += ch.T * d;
         }
-        bound += size[j] * dur[j];
+        for (double l : t0) planned = std::max(planned, l);
+        base += ch.T * (int)ch.load.size();
     }
     std::stable_sort(placed.begin(), placed.end(), [](const Placed& x, const Placed& y) {
         if (x.cta != y.cta) return x.cta < y.cta;
@@ -2255,7 +2320,6 @@ static int team_schedule(const std::vector<int>& n, const std::vector<int>& U, i
         begin[placed[t].cta + 1]++;
     }
     for (int b = 0; b < G; ++b) begin[b + 1] += begin[b];
-    planned = J ? *std::max_element(avail.begin(), avail.end()) : 0.0;
     bound /= G;
     return SCFT_OK;
 }
@@ -2276,7 +2340,7 @@ struct scft_batch_s {
     // Form 4: the contours of every instance whose own plan is the alternating FP64 kernel
     // run in ONE persistent launch of batch_contour_kernel (contour_batch.cuh); the
     // instances' prep and field kernels stay on the worker streams before and after it.
-    double team_balance = 1.0;      // a chain's team grows until it lasts <= balance x the mean load
+    std::map<int, int> team_fixed;  // grid side -> team size set by the caller (else the planner's choice)
     std::vector<char> in_team;      // per instance: its contour runs in the batch kernel
     DevBuf<TeamChain> team_chains;
     DevBuf<TeamTask> team_tasks;
@@ -2330,7 +2394,7 @@ struct scft_batch_s {
         std::vector<TeamTask> tasks;
         std::vector<int> begin;
         double planned = 0.0, bound = 0.0;
-        CKR(team_schedule(side, steps, G, team_balance, size, tasks, begin, planned, bound));
+        CKR(team_schedule(side, steps, G, team_fixed, size, tasks, begin, planned, bound));
 
         // chain descriptors (tensor maps of each instance's stores and Boltzmann factors)
         size_t nflags = 0;
@@ -2624,22 +2688,17 @@ int scft_batch_autotune(scft_batch_t b, size_t n_trial, size_t* best_nstreams, i
         std::vector<std::vector<double>> keepA, keepB;
         size_t ns0;
         int form0;
-        double balance0;
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         bool keep_config = false;
         ~Guard() {
             if (e0) cudaEventDestroy(e0);
             if (e1) cudaEventDestroy(e1);
             cudaStreamSynchronize(b->main);
-            if (!keep_config) {
-                scft_batch_configure(b, ns0, form0);
-                b->team_balance = balance0;
-            }
+            if (!keep_config) scft_batch_configure(b, ns0, form0);
             for (size_t i = 0; i < keepA.size(); ++i)
                 if (!keepA[i].empty()) scft_diblock_set_fields(b->runs[i], keepA[i].data(), keepB[i].data());
         }
-    } g{b, std::vector<std::vector<double>>(n), std::vector<std::vector<double>>(n), b->nstreams, b->form,
-        b->team_balance};
+    } g{b, std::vector<std::vector<double>>(n), std::vector<std::vector<double>>(n), b->nstreams, b->form};
     for (size_t i = 0; i < n; ++i) {
         std::vector<double> a(b->runs[i]->M), bb(b->runs[i]->M);
         CKR(scft_diblock_get_fields(b->runs[i], nullptr, nullptr, a.data(), bb.data()));
@@ -2651,43 +2710,29 @@ int scft_batch_autotune(scft_batch_t b, size_t n_trial, size_t* best_nstreams, i
     double best = 1e300;
     size_t bs = b->nstreams;
     int bf = b->form;
-    double bb = b->team_balance;
     const size_t cand_streams[] = {2, 4, 8, 16, 32};
     const int cand_forms[] = {0, 2, 4};
-    // form 4: the team-size balance (how long a chain may run against the mean load of a CTA)
-    const double cand_balance[] = {0.5, 1.0, 2.0};
-    auto trial = [&](size_t ns, int f, double balance) -> int {
-        CKR(scft_batch_configure(b, ns, f));
-        b->team_balance = balance;
-        CKR(b->run(1, nullptr, nullptr));  // capture + warm up
-        CK(cudaEventRecord(g.e0, b->main));
-        CKR(b->run(n_trial, nullptr, nullptr));
-        CK(cudaEventRecord(g.e1, b->main));
-        CK(cudaEventSynchronize(g.e1));
-        float ms = 0.f;
-        CK(cudaEventElapsedTime(&ms, g.e0, g.e1));
-        if (ms < best) {
-            best = ms;
-            bs = ns;
-            bf = f;
-            bb = balance;
-        }
-        return SCFT_OK;
-    };
     for (int f : cand_forms) {
         for (size_t ns : cand_streams) {
             if (ns > n && ns != cand_streams[0]) continue;
-            if (f == 4) {
-                // the worker streams only carry the small per-instance kernels here
-                if (ns != 4 && ns != 16) continue;
-                for (double bal : cand_balance) CKR(trial(ns, f, bal));
-            } else {
-                CKR(trial(ns, f, b->team_balance));
+            // form 4: the worker streams only carry the small per-instance kernels
+            if (f == 4 && ns != 4 && ns != 16) continue;
+            CKR(scft_batch_configure(b, ns, f));
+            CKR(b->run(1, nullptr, nullptr));  // capture + warm up
+            CK(cudaEventRecord(g.e0, b->main));
+            CKR(b->run(n_trial, nullptr, nullptr));
+            CK(cudaEventRecord(g.e1, b->main));
+            CK(cudaEventSynchronize(g.e1));
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, g.e0, g.e1));
+            if (ms < best) {
+                best = ms;
+                bs = ns;
+                bf = f;
             }
         }
     }
     CKR(scft_batch_configure(b, bs, bf));
-    b->team_balance = bb;
     g.keep_config = true;  // the guard now only restores the fields and frees the events
     if (best_nstreams) *best_nstreams = bs;
     if (best_form) *best_form = bf;
@@ -2695,15 +2740,18 @@ int scft_batch_autotune(scft_batch_t b, size_t n_trial, size_t* best_nstreams, i
     return SCFT_OK;
 }
 
-int scft_team_schedule(size_t nchains, const int* n, const int* U, int G, double balance, int* size, size_t cap,
-                       int* task_chain, int* task_rank, int* task_size, int* task_begin, size_t* ntasks,
-                       double* planned_us, double* bound_us) {
-    if (!n || !U || !size || !task_begin || !ntasks) return fail(SCFT_ERR_INVALID_ARG, "null argument");
+int scft_team_schedule(size_t nchains, const int* n, const int* U, int G, size_t nfixed, const int* fixed_sides,
+                       const int* fixed_sizes, int* size, size_t cap, int* task_chain, int* task_rank,
+                       int* task_size, int* task_begin, size_t* ntasks, double* planned_us, double* bound_us) {
+    if (!n || !U || !size || !task_begin || !ntasks || (nfixed && (!fixed_sides || !fixed_sizes)))
+        return fail(SCFT_ERR_INVALID_ARG, "null argument");
     std::vector<int> vn(n, n + nchains), vu(U, U + nchains), sz;
+    std::map<int, int> fixed;
+    for (size_t i = 0; i < nfixed; ++i) fixed[fixed_sides[i]] = fixed_sizes[i];
     std::vector<TeamTask> tasks;
     std::vector<int> begin;
     double planned = 0.0, bound = 0.0;
-    CKR(team_schedule(vn, vu, G, balance, sz, tasks, begin, planned, bound));
+    CKR(team_schedule(vn, vu, G, fixed, sz, tasks, begin, planned, bound));
     *ntasks = tasks.size();
     if (tasks.size() > cap || ((!task_chain || !task_rank || !task_size) && !tasks.empty()))
         return fail(SCFT_ERR_INVALID_ARG, "team schedule: task arrays too small (" + std::to_string(tasks.size()) +
@@ -2720,12 +2768,16 @@ int scft_team_schedule(size_t nchains, const int* n, const int* U, int G, double
     return SCFT_OK;
 }
 
-int scft_batch_set_team_balance(scft_batch_t b, double balance) {
-    if (!b || !(balance > 0.0)) return fail(SCFT_ERR_INVALID_ARG, "bad argument");
+int scft_batch_set_team_sizes(scft_batch_t b, size_t count, const int* sides, const int* sizes) {
+    if (!b || (count && (!sides || !sizes))) return fail(SCFT_ERR_INVALID_ARG, "null argument");
+    for (size_t i = 0; i < count; ++i)
+        if (sides[i] < 1 || sizes[i] < 1 || sides[i] % sizes[i])
+            return fail(SCFT_ERR_INVALID_ARG, "a team size must divide its grid side");
     CK(cudaSetDevice(b->device));
     CK(cudaStreamSynchronize(b->main));
     b->drop_graph();
-    b->team_balance = balance;
+    b->team_fixed.clear();
+    for (size_t i = 0; i < count; ++i) b->team_fixed[sides[i]] = sizes[i];
     return SCFT_OK;
 }
 

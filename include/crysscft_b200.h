@@ -278,10 +278,10 @@ int scft_batch_iterate(scft_batch_t b, size_t n_iter, double* F, double* maxinc)
  * on a team of CTAs that own several x-planes / y-slabs each; the other instances keep
  * their own kernels).  Forms 0-3 launch one contour kernel per instance. */
 int scft_batch_configure(scft_batch_t b, size_t nstreams, int form);
-/* Form 4: a chain's team grows (next divisor of its grid side) while the chain would last
- * longer than `balance` x the mean load of a CTA under the planner's cost model; smaller
- * balances give larger teams (shorter chains, more exchange overhead).  Default 1. */
-int scft_batch_set_team_balance(scft_batch_t b, double balance);
+/* Form 4: fixed team sizes for the listed grid sides (sizes[i] must divide sides[i]);
+ * chains of other sides get the planner's choice (scft_team_schedule).  count 0 clears
+ * the table. */
+int scft_batch_set_team_sizes(scft_batch_t b, size_t count, const int* sides, const int* sizes);
 /* The form-4 plan of the current configuration (built if needed): CTAs of the launch (0 if
  * no instance runs in it), team tasks, instances in the launch, and the planned makespan
  * and the lower bound (team work / CTAs) in microseconds per iteration under the cost
@@ -289,15 +289,19 @@ int scft_batch_set_team_balance(scft_batch_t b, double balance);
 int scft_batch_team_plan(scft_batch_t b, int* grid, size_t* ntasks, size_t* ninstances, double* planned_us,
                          double* bound_us);
 /* The form-4 planner on the host alone (no GPU): nchains chains with grid side n[j] and
- * U[j] contour steps on G CTAs.  size[j] receives each chain's team size; the tasks
+ * U[j] contour steps on G CTAs; nfixed grid sides with team sizes fixed by the caller
+ * (may be 0).  Chains of one grid side form a class; for a target makespan a class with
+ * team size T runs in columns of T CTAs with its chains stacked in them, and takes the T
+ * that needs fewest CTAs; the smallest target whose classes fit in G CTAs is kept.
+ * size[j] receives each chain's team size; the tasks
  * (chain, rank in team, team size), grouped by CTA, go to task_chain/task_rank/task_size
  * (room for cap), CTA b's tasks being [task_begin[b], task_begin[b + 1]) (G + 1 entries);
  * *ntasks receives the count (also when cap is too small, which returns
  * SCFT_ERR_INVALID_ARG).  planned_us / bound_us: makespan and its lower bound per
  * iteration under the planner's cost model.  No counterpart in the reference. */
-int scft_team_schedule(size_t nchains, const int* n, const int* U, int G, double balance, int* size, size_t cap,
-                       int* task_chain, int* task_rank, int* task_size, int* task_begin, size_t* ntasks,
-                       double* planned_us, double* bound_us);
+int scft_team_schedule(size_t nchains, const int* n, const int* U, int G, size_t nfixed, const int* fixed_sides,
+                       const int* fixed_sizes, int* size, size_t cap, int* task_chain, int* task_rank,
+                       int* task_size, int* task_begin, size_t* ntasks, double* planned_us, double* bound_us);
 /* Kernel launches of one batch iteration in the current configuration. */
 int scft_batch_launches_per_iteration(scft_batch_t b, size_t* n);
 /* Time n_trial batch iterations for each candidate configuration, keep the fastest.

@@ -80,11 +80,11 @@ def _mixed(n=10, seed=11):
     return cfg
 
 
-@pytest.mark.parametrize("balance", [0.25, 1.0, 4.0])
-def test_one_launch_form_is_bit_identical_to_per_instance_kernels(gpu, balance):
+@pytest.mark.parametrize("teams", [None, {16: 1, 24: 1, 32: 1, 48: 1, 64: 1}, {16: 16, 24: 12, 32: 8, 48: 6, 64: 32}])
+def test_one_launch_form_is_bit_identical_to_per_instance_kernels(gpu, teams):
     # form 4 runs each chain on a team of CTAs that own several planes / slabs each; every
     # unit does the per-instance kernel's arithmetic in the same order, so the results are
-    # the same bits whatever the team sizes (balance 4: one CTA per chain at every size)
+    # the same bits whatever the team sizes (the planner's, one CTA per chain, wide teams)
     inst = _mixed()
     B1 = batch.BatchSCFT("PMMM", inst)
     B1.configure(4, 1)
@@ -92,7 +92,8 @@ def test_one_launch_form_is_bit_identical_to_per_instance_kernels(gpu, balance):
     h1 = B1.iterate(3)
     B4 = batch.BatchSCFT("PMMM", inst)
     B4.configure(4, 4)
-    B4.set_team_balance(balance)
+    if teams:
+        B4.set_team_sizes(teams)
     B4.seed_fields()
     plan = B4.team_plan()
     assert plan["instances"] == len(inst) and plan["grid"] > 0
