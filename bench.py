@@ -38,6 +38,8 @@ def parse():
     ap.add_argument("--solver", choices=["PMMM", "3M", "P1"], default="PMMM")
     ap.add_argument("--grid", type=int, default=128)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra-legs", action="store_true",
+                    help="skip the batch and 256^3 legs of the default run")
     ap.add_argument("--workload", choices=["single", "batch"], default="single",
                     help="single: the 128^3 BCC system; batch: 64 seeded PMMM instances of mixed size")
     ap.add_argument("--instances", type=int, default=64)
@@ -259,6 +261,71 @@ def drop_in_triplets(solver, stream, M: int, n_dev: int = 400, n_host: int = 100
                             "per triplet)"}
 
 
+def batch_leg(local: int, steps: int = 10):
+    """The batching form on its configured workload (64 PMMM instances, reduced grids
+    {16..64}^3, ds = 0.01): the contours of all instances in one persistent launch (form 4)
+    and, for comparison, one contour kernel per instance (form 0).  Wall-timed around
+    synchronous batch iterations (each ends with the per-instance history copies)."""
+    import torch
+
+    from crysscft_sample_b200 import batch
+
+    cfg = batch.batch_config(64)
+    B = batch.BatchSCFT("PMMM", cfg, ds=0.01, device=local)
+    B.seed_fields()
+    out = {"workload": "64 PMMM instances, reduced grids from {16,24,32,48,64}^3, chiN~U[14,30], "
+                       "fA~U[0.2,0.35], L~U[3.8,5.5], ds=0.01, BCC or FCC (seeded)",
+           "unit": "instance-iterations/s", "steps": steps}
+    for form, ns, key in ((4, 4, "one_launch"), (0, 8, "per_instance_kernels")):
+        B.configure(ns, form)
+        B.iterate(3)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        B.iterate(steps)
+        dt = time.perf_counter() - t0
+        out[key] = {"value": len(cfg) * steps / dt, "ms_per_iteration": dt / steps * 1e3,
+                    "launches_per_iteration": B.launches_per_iteration()}
+        if form == 4:
+            out[key]["plan"] = B.team_plan()
+    out["speedup"] = out["one_launch"]["value"] / out["per_instance_kernels"]["value"]
+    B.close()
+    return out
+
+
+def grid256_leg(local: int, stream, steps: int = 10):
+    """The same BCC system on the 256^3 full grid (PmmmDCT on 128^3, Ns = 200), FP64 and FP32
+    triplets, CUDA events on the library's stream around `steps` iterations each."""
+    import torch
+
+    from crysscft_sample_b200 import fields, scft, solvers
+
+    n = 256
+    N = (n, n, n)
+    L = WORKLOAD["L"]
+    G = solvers.make_solver("PMMM", N, precision="fp64", device=local)
+    G.set_stream(stream)
+    G.set_cell_para((L, L, L))
+    run = scft.DiblockSCFT(G, WORKLOAD["fA"], WORKLOAD["ds"], WORKLOAD["xN"], WORKLOAD["acc"])
+    wA, wB = fields.seed_fields(N, L, WORKLOAD["phase"], seed=20261203)
+    run.set_fields(fields.to_physical("PMMM", wA), fields.to_physical("PMMM", wB))
+    out = {"workload": "AB diblock BCC 256^3 full grid, PMMM solver on 128^3, Ns=200 (ds=0.005)",
+           "unit": "iterations/s", "steps": steps}
+    for prec in ("fp64", "fp32"):
+        run.set_precision(prec)
+        run.iterate(3)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        run.iterate(steps)
+        e1.record(stream)
+        e1.synchronize()
+        out[prec] = {"value": steps / (e0.elapsed_time(e1) / 1e3)}
+    out["fp32_speedup"] = out["fp32"]["value"] / out["fp64"]["value"]
+    run.close()
+    G.close()
+    return out
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -376,6 +443,11 @@ def run_ours(args):
 
     # ---- the drop-in per-triplet boundary (CrysPSSolverBase::diffusion) ----
     drop_in = drop_in_triplets(solver, stream, M)
+    # ---- the batching form and the 256^3 size on the default run -------------
+    extra = {}
+    if args.grid == 128 and args.solver == "PMMM" and not args.no_extra_legs:
+        extra["batch_form"] = batch_leg(local)
+        extra["grid256"] = grid256_leg(local, stream)
     # per triplet: read q(s), read exp(-w ds/2), write q(s+1); K generated on chip, not counted
     alg_bytes_launch = 2 * U * 3 * M * b
     achieved = alg_bytes_launch / chain_s / 1e9
@@ -456,6 +528,7 @@ def run_ours(args):
             "F_last": float(hist["F"][-1]),
             "precision_form": precision_form,
             "drop_in": drop_in,
+            **extra,
         }
     if dist is not None:
         dist.barrier()
