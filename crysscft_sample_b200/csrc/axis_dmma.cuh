@@ -24,6 +24,57 @@ namespace crysscft {
 constexpr int kRowsZ = 32;
 constexpr int kColsYX = 32;
 
+// L2 eviction priorities of the pass traffic.  At 256^3 the two chains' working set (the
+// Boltzmann factors, the field a pass reads and the one it writes) is close to the L2
+// size, and the contour slices written every step stream through it.  A pass's output
+// is read by the next pass (evict_last); its input is dead once read (evict_first, which
+// also demotes the line the previous pass kept); the Boltzmann factors are reused every
+// step (evict_last).  hints == 0 issues the plain cache-global forms.
+// Drop the 128-byte L2 line at a (128-byte aligned) without writing it back: for a pass
+// input that no one reads again (the triplet's intermediate fields), so that evicting
+// it costs no DRAM write.
+__device__ __forceinline__ void l2_discard_line(const void* a) {
+    asm volatile("discard.global.L2 [%0], 128;" ::"l"(a) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long l2_policy(bool last) {
+    unsigned long long p;
+    if (last) asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    else asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ double2 ld_cg_policy(const double* a, unsigned long long pol) {
+    double2 v;
+    asm volatile("ld.global.cg.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(v.x), "=d"(v.y) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ double2 ld_nc_policy(const double* a, unsigned long long pol) {
+    double2 v;
+    asm volatile("ld.global.nc.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(v.x), "=d"(v.y) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ void st_cg_policy(double* a, double2 v, unsigned long long pol) {
+    asm volatile("st.global.cg.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;" ::"l"(a), "d"(v.x), "d"(v.y), "l"(pol)
+                 : "memory");
+}
+__device__ __forceinline__ float4 ld_cg_policy(const float* a, unsigned long long pol) {
+    float4 v;
+    asm volatile("ld.global.cg.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ float4 ld_nc_policy(const float* a, unsigned long long pol) {
+    float4 v;
+    asm volatile("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ void st_cg_policy(float* a, float4 v, unsigned long long pol) {
+    asm volatile("st.global.cg.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;" ::"l"(a), "f"(v.x), "f"(v.y),
+                 "f"(v.z), "f"(v.w), "l"(pol)
+                 : "memory");
+}
+
 struct AxisPassD {
     const double* in[2];
     double* out[2];
@@ -31,6 +82,9 @@ struct AxisPassD {
     const double* post[2];  // x pass: output *= post (nullptr: none)
     const double* op;       // this axis' packed operator (AxisShape<N, EO> or AxisShapeEO2<N> layout)
     int nchain;
+    int hints;              // 1: L2 eviction priorities on the pass traffic (see l2_policy)
+    int discard_in;         // 1: the input is dead once read (a triplet intermediate): drop its
+                            // L2 lines after the tile is loaded (y and x passes)
 };
 
 template <int N, bool EO, bool EO2 = false>
@@ -77,6 +131,7 @@ __global__ void __launch_bounds__(kContourThreads, 1) axis_dmma_kernel(const Axi
     op_copy_async(sop, p.op, S::OP_VALUES);
 
     const int tiles = p.nchain * TL::TILES_PER_CHAIN;
+    const unsigned long long pol_first = l2_policy(false), pol_last = l2_policy(true);
     double2 v[PT], w[PT];
     // fetch tile t into registers (input x pre for the z pass; post for the x pass)
     auto fetch = [&](int t) {
@@ -89,8 +144,13 @@ __global__ void __launch_bounds__(kContourThreads, 1) axis_dmma_kernel(const Axi
             const int e = (k * kContourThreads + threadIdx.x) * 2;
             const int r = e / RL, cc = e - r * RL;
             const long long g = r * TL::ROW_STRIDE + cc;
-            v[k] = __ldcg(reinterpret_cast<const double2*>(in + g));
-            if (aux) w[k] = __ldg(reinterpret_cast<const double2*>(aux + o + g));
+            if (p.hints) {
+                v[k] = ld_cg_policy(in + g, pol_first);
+                if (aux) w[k] = ld_nc_policy(aux + o + g, pol_last);
+            } else {
+                v[k] = __ldcg(reinterpret_cast<const double2*>(in + g));
+                if (aux) w[k] = __ldg(reinterpret_cast<const double2*>(aux + o + g));
+            }
         }
     };
     int t = blockIdx.x;
@@ -119,6 +179,15 @@ __global__ void __launch_bounds__(kContourThreads, 1) axis_dmma_kernel(const Axi
             for (int k = 0; k < PT; ++k) wpost[k] = w[k];
         }
         __syncthreads();
+        if (AX != 2 && p.discard_in) {
+            // every load of this tile has returned (its values are in F): drop the input's
+            // lines, two 128-byte lines per tile row of kColsYX doubles
+            constexpr int LINES = N * (kColsYX * (int)sizeof(double) / 128);
+            if (threadIdx.x < LINES) {
+                const int r = threadIdx.x / (LINES / N), h = threadIdx.x - r * (LINES / N);
+                l2_discard_line(p.in[c] + o + r * TL::ROW_STRIDE + h * (128 / (int)sizeof(double)));
+            }
+        }
         if (t + (int)gridDim.x < tiles) fetch(t + gridDim.x);  // in flight during the MMAs
         if constexpr (AX == 2) {
             if constexpr (EO2) row_op_eo2<kRowsZ, N, LF>(F, G, sop);
@@ -138,7 +207,8 @@ __global__ void __launch_bounds__(kContourThreads, 1) axis_dmma_kernel(const Axi
                 y.x *= wpost[k].x;
                 y.y *= wpost[k].y;
             }
-            __stcg(reinterpret_cast<double2*>(out + r * TL::ROW_STRIDE + cc), y);
+            if (p.hints) st_cg_policy(out + r * TL::ROW_STRIDE + cc, y, pol_last);
+            else __stcg(reinterpret_cast<double2*>(out + r * TL::ROW_STRIDE + cc), y);
         }
     }
 }
@@ -151,6 +221,8 @@ struct AxisPassF {
     const float* post[2];
     const float* op;  // this axis' packed TF32 hi/lo operator (AxisShapeF<N, EO> layout)
     int nchain;
+    int hints;        // as AxisPassD::hints
+    int discard_in;   // as AxisPassD::discard_in
 };
 
 template <int N, bool EO>
@@ -179,6 +251,7 @@ __global__ void __launch_bounds__(kContourThreads) axis_tf32_kernel(const AxisPa
     op_copy_async(sop, p.op, AxisShapeF<N, EO>::SIZE);
 
     const int tiles = p.nchain * TL::TILES_PER_CHAIN;
+    const unsigned long long pol_first = l2_policy(false), pol_last = l2_policy(true);
     float4 v[PT], w[PT];
     auto fetch = [&](int t) {
         const int c = t / TL::TILES_PER_CHAIN;
@@ -190,8 +263,13 @@ __global__ void __launch_bounds__(kContourThreads) axis_tf32_kernel(const AxisPa
             const int e = (k * kContourThreads + threadIdx.x) * 4;
             const int r = e / RL, cc = e - r * RL;
             const long long g = r * TL::ROW_STRIDE + cc;
-            v[k] = __ldcg(reinterpret_cast<const float4*>(in + g));
-            if (aux) w[k] = __ldg(reinterpret_cast<const float4*>(aux + o + g));
+            if (p.hints) {
+                v[k] = ld_cg_policy(in + g, pol_first);
+                if (aux) w[k] = ld_nc_policy(aux + o + g, pol_last);
+            } else {
+                v[k] = __ldcg(reinterpret_cast<const float4*>(in + g));
+                if (aux) w[k] = __ldg(reinterpret_cast<const float4*>(aux + o + g));
+            }
         }
     };
     int t = blockIdx.x;
@@ -222,6 +300,10 @@ __global__ void __launch_bounds__(kContourThreads) axis_tf32_kernel(const AxisPa
             for (int k = 0; k < PT; ++k) wpost[k] = w[k];
         }
         __syncthreads();
+        if (AX != 2 && p.discard_in) {  // as in axis_dmma_kernel: one 128-byte line per tile row
+            static_assert(kColsYX * sizeof(float) == 128, "one line per FP32 tile row");
+            if (threadIdx.x < N) l2_discard_line(p.in[c] + o + threadIdx.x * TL::ROW_STRIDE);
+        }
         if (t + (int)gridDim.x < tiles) fetch(t + gridDim.x);
         if constexpr (AX == 2) row_op_f32<kRowsZ, N, LF, EO>(F, G, sop);
         else col_op_f32<N, kColsYX, LF, EO>(F, G, sop);
@@ -238,7 +320,8 @@ __global__ void __launch_bounds__(kContourThreads) axis_tf32_kernel(const AxisPa
                 y.z *= wpost[k].z;
                 y.w *= wpost[k].w;
             }
-            __stcg(reinterpret_cast<float4*>(out + r * TL::ROW_STRIDE + cc), y);
+            if (p.hints) st_cg_policy(out + r * TL::ROW_STRIDE + cc, y, pol_last);
+            else __stcg(reinterpret_cast<float4*>(out + r * TL::ROW_STRIDE + cc), y);
         }
     }
 }

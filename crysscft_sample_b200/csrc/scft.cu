@@ -55,6 +55,16 @@ int fail(int code, const std::string& msg) {
         if (r_ != SCFT_OK) return r_;      \
     } while (0)
 
+// L2 eviction priorities on the tensor-core axis passes (axis_dmma.cuh); off with
+// CRYSSCFT_L2_HINTS=0 (read once).
+int l2_hints_enabled() {
+    static const int on = [] {
+        const char* e = getenv("CRYSSCFT_L2_HINTS");
+        return (e && e[0] == '0') ? 0 : 1;
+    }();
+    return on;
+}
+
 // TMA descriptor encoder of the driver (cuTensorMapEncodeTiled), resolved once.
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -873,6 +883,8 @@ struct scft_solver_s {
                         px.in[c] = t2[c]; px.out[c] = io[c].out; px.post[c] = io[c].post;
                     }
                     pz.nchain = py.nchain = px.nchain = nchain;
+                    pz.hints = py.hints = px.hints = l2_hints_enabled();
+                    py.discard_in = px.discard_in = l2_hints_enabled();  // t1, t2: dead once read
                     if (eo2) {
                         const size_t per_axis = ops->h_packed2.size() / 3;  // AxisShapeEO2<n>::SIZE
                         pz.op = ops->d_packed2.p + 2 * per_axis;
@@ -918,6 +930,8 @@ struct scft_solver_s {
                         px.post[c] = (const float*)io[c].post;
                     }
                     pz.nchain = py.nchain = px.nchain = nchain;
+                    pz.hints = py.hints = px.hints = l2_hints_enabled();
+                    py.discard_in = px.discard_in = l2_hints_enabled();  // t1, t2: dead once read
                     pz.op = ops->f_packed.p + 2 * stride;
                     py.op = ops->f_packed.p + stride;
                     px.op = ops->f_packed.p;
