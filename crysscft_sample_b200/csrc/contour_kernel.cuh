@@ -1069,10 +1069,20 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
         }
         cp_async_commit();
         cp_async_wait_all();
-        __syncthreads();
-        if (s_fail) {
-            drain(true);
-            return;
+        if (EO2 && plane && k >= 1) {
+            static_assert(!EO2 || (TPR == 4 && AxisShapeEO2<N>::GROUPS == 2),
+                          "warp w fetches rows 8w..8w+7; row_op_eo2 gives warps 2b, 2b+1 rows 16b..16b+15");
+            // the first operation (A_z along rows) of warps 2b, 2b+1 reads only rows
+            // 16b..16b+15, which these two warps fetched: they start as soon as their own
+            // producers' rows are in, while other rows are still arriving.  A wait that ran
+            // out is caught at the block barrier after the operation.
+            asm volatile("bar.sync %0, 64;" ::"r"(1 + (warp >> 1)) : "memory");
+        } else {
+            __syncthreads();
+            if (s_fail) {
+                drain(true);
+                return;
+            }
         }
         double* cur = T0;
         double* oth = T1;
