@@ -173,3 +173,45 @@ def test_batching_configuration_200_iterations(gpu):
                                                        fields.to_physical("PMMM", wB))
         rel = np.abs(hb["F"][:, i] - want["F"]) / np.abs(want["F"])
         assert rel.max() <= 1e-10, f"instance {i} ({it['N']}) vs reference: max |dF/F| {rel.max():.3e}"
+
+
+def _run_forms(kind, inst, precision="fp64", n_iter=3):
+    out = []
+    for form in (1, 4):
+        B = batch.BatchSCFT(kind, inst, precision=precision)
+        B.configure(4, form)
+        B.seed_fields()
+        h = B.iterate(n_iter)
+        plan = B.team_plan()
+        fields_ = [B.get_fields(i) for i in range(len(inst))]
+        B.close()
+        out.append((h, plan, fields_))
+    return out
+
+
+def test_one_launch_form_with_instances_it_cannot_take(gpu):
+    # physical 12^3 (not a multiple of 8) has no alternating kernel: that instance keeps its
+    # own kernels on a worker stream, the others go to the one launch; the results match
+    inst = _mixed(6, seed=13)
+    inst[1]["N"] = (24, 24, 24)
+    (h1, _, f1), (h4, plan, f4) = _run_forms("PMMM", inst)
+    assert plan["instances"] == len(inst) - 1
+    assert np.array_equal(h4["F"], h1["F"])
+    for a, b in zip(f1, f4):
+        assert all(np.array_equal(a[k], b[k]) for k in a)
+
+
+def test_one_launch_form_p1_batch(gpu):
+    # P1 (one even/odd level on every axis) through the same batch kernel
+    inst = batch.batch_config(4, seed=21, sizes=(8, 16, 24, 32))
+    (h1, _, _), (h4, plan, _) = _run_forms("P1", inst)
+    assert plan["instances"] == len(inst)
+    assert np.array_equal(h4["F"], h1["F"])
+
+
+def test_one_launch_form_leaves_fp32_instances_to_their_kernels(gpu):
+    # the batch kernel is FP64; an FP32 batch in form 4 plans no team and runs as form 0
+    inst = _mixed(5, seed=17)
+    (h1, _, _), (h4, plan, _) = _run_forms("PMMM", inst, precision="fp32")
+    assert plan["instances"] == 0 and plan["grid"] == 0
+    assert np.array_equal(h4["F"], h1["F"])
