@@ -3,15 +3,15 @@
 //
 // Each chain (forward q or backward q+ of one instance, src/crysSCFT_sample.cpp:483-491)
 // runs on a team of T CTAs with the alternating-layout schedule of contour_alt_kernel
-// (plane phase [A_z A_y] D store D [A_z A_y], slab phase [A_x] D store D [A_x], one
+// (plane phase [A_z A_y] D store D [A_y], slab phase [A_z A_x] D store D [A_x], one
 // exchange per step through the chain's exchange buffers).  Where contour_alt_kernel gives
 // every unit (x-plane or y-slab) its own CTA, a team CTA owns P = n / T units (rank,
 // rank + T, ...) and runs them one after the other in every phase, so a chain occupies T
 // SMs instead of n and one exchange latency per step is shared by P units of work.
 // Synchronisation is per phase and CTA pair: a CTA waits once per phase for one flag of
 // every producer CTA of its team, and releases its own flags once, after its last unit;
-// while the last axis operation of a unit runs, the next unit's tile is fetched into the
-// work tile that operation no longer reads.  Every unit does exactly the arithmetic of
+// while a unit's last axis operation runs, the next unit's tile is fetched into the work
+// tile the unit no longer reads.  Every unit does exactly the arithmetic of
 // contour_alt_kernel (same tile operations and epilogues, in the same order), so the
 // results are bit-identical to the per-instance kernel.
 //
@@ -108,7 +108,7 @@ __device__ bool team_chain(const BatchContourArgs& a, const TeamChain* ch, int r
                 atomicOr(err, (unsigned)e);
                 atomicOr(a.abort, 1u);
             }
-            return false;
+            return false;  // the kernel lets the earlier tasks' q stores finish before it leaves
         }
     }
     if (threadIdx.x == 0) {
@@ -168,14 +168,16 @@ __device__ bool team_chain(const BatchContourArgs& a, const TeamChain* ch, int r
         else col_op_ct<N, N, LF, EO, kToGlobal>(F, o, sops + off);
     };
 
-    // unit j's tile of phase k into T0: the contour store's input slice in phase 0, else
-    // the rows the other layout wrote to its exchange buffer in phase k-1
+    // unit j's tile of phase k into its work tile (T0 for even j, T1 for odd j: a unit's
+    // second work tile is free once its finishing operation has run, and takes the next
+    // unit's tile): the contour store's input slice in phase 0, else the rows the other
+    // layout wrote to its exchange buffer in phase k-1
     auto fetch = [&](int k, int j) {
         const bool plane = (k & 1) == 0;
         const int p = rank + j * T;
         const long long off = plane ? (long long)p * PLANE : (long long)p * N;
         const long long gs = plane ? N : PLANE;
-        tile_fetch<N, LF>(T0, (k == 0 ? q + slot0 * M : (plane ? XS : XP)) + off, gs);
+        tile_fetch<N, LF>((j & 1) ? T1 : T0, (k == 0 ? q + slot0 * M : (plane ? XS : XP)) + off, gs);
         cp_async_commit();
     };
 
@@ -210,40 +212,34 @@ __device__ bool team_chain(const BatchContourArgs& a, const TeamChain* ch, int r
             const int p = rank + j * T;
             const long long off = plane ? (long long)p * PLANE : (long long)p * N;
             const long long gs = plane ? N : PLANE;
-            const bool more = j + 1 < P;  // prefetch unit j+1 into T0 once T0 is free
+            const bool more = j + 1 < P;  // prefetch unit j+1 into `oth` once it is free
             cp_async_wait_all();
             __syncthreads();
-            double* cur = T0;
-            double* oth = T1;
+            double* cur = (j & 1) ? T1 : T0;
+            double* oth = (j & 1) ? T0 : T1;
             if (k >= 1) {
-                // finish step k-1 on this unit; the last op's epilogue applies D, writes
-                // q(s+1) to the staging tile and D q(s+1) to the work tile
-                if (plane) row_z(cur, oth);
+                // finish step k-1 on this unit (A_z, then the layout's column axis, whose
+                // epilogue applies D, writes q(s+1) to the staging tile and D q(s+1) to cur),
+                // as contour_alt_kernel
+                row_z(cur, oth);
                 if (warp == 0) bulk_wait_read();  // the previous q store has left QS
                 if (!mbar_wait(bar, wpar, a.spin_limit)) *s_fail = 1;
                 __syncthreads();
                 if (*s_fail) return fail_exit(2u, true);
                 wpar ^= 1u;
-                ColOut fo{plane ? cur : oth, 0};
+                ColOut fo{cur, 0};
                 fo.w0 = W0;
                 fo.w1 = W1;
                 fo.qs = QS;
                 fo.start = k < U;
-                if constexpr (EO2) col_op_eo2<N, N, LF, kFinish>(plane ? oth : cur, fo, sops + (plane ? OFFY : 0));
-                else col_op_ct<N, N, LF, EO, kFinish>(plane ? oth : cur, fo, sops + (plane ? OFFY : 0));
-                if (!plane) {
-                    double* tmp = cur;
-                    cur = oth;
-                    oth = tmp;
-                }
+                if constexpr (EO2) col_op_eo2<N, N, LF, kFinish>(oth, fo, sops + (plane ? OFFY : 0));
+                else col_op_ct<N, N, LF, EO, kFinish>(oth, fo, sops + (plane ? OFFY : 0));
                 fence_async_smem();
                 __syncthreads();
                 if (threadIdx.x == 0) {
                     tma_store_5d(&ch->tm_q[plane ? 0 : 1], QS, 0, 0, 0, p, (int)(slot0 + (long long)dir * k));
                     bulk_commit();
                 }
-                // last phase (nothing started) or slab phase (the work tile is now T1): T0 is free
-                if (more && (k == U || !plane)) fetch(k, j + 1);
             } else {
                 if (!mbar_wait(bar, wpar, a.spin_limit)) *s_fail = 1;
                 __syncthreads();
@@ -252,22 +248,17 @@ __device__ bool team_chain(const BatchContourArgs& a, const TeamChain* ch, int r
                 tile_scale_panel<N, LF>(cur, W1);
                 __syncthreads();
             }
+            if (more) fetch(k, j + 1);  // into oth, which nothing reads any more this unit
             // W0/W1 are free: prefetch the factors of the next (phase, unit)
             if (warp == 0) {
                 if (more) issue_w(k, p + T);
                 else if (k < U) issue_w(k + 1, rank);
             }
             if (k < U) {
-                // start step k on this unit; the last op's epilogue writes the exchange buffer
+                // start step k on this unit with the layout's column axis; the epilogue
+                // writes the exchange buffer
                 const ColOut xo{(plane ? XP : XS) + off, gs};
-                if (plane) {
-                    row_z(cur, oth);
-                    __syncthreads();
-                    if (more) fetch(k, j + 1);  // T0 (cur) has been read
-                    col_global(oth, xo, OFFY);
-                } else {
-                    col_global(cur, xo, 0);
-                }
+                col_global(cur, xo, plane ? OFFY : 0);
             }
         }
         __syncthreads();
@@ -316,8 +307,10 @@ __global__ void __launch_bounds__(kContourThreads, 1) batch_contour_kernel(const
                 }
                 break;
         }
-        if (!ok) return;
+        if (!ok) break;
     }
+    // the q stores of the last tasks (or of the tasks before a failure) read shared memory
+    // until they complete: wait for them before the block leaves
     if ((threadIdx.x >> 5) == 0) bulk_wait_all();
 }
 

@@ -813,8 +813,11 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_kernel_ct(const Co
 // ---------------------------------------------------------------------------
 // Alternating-layout schedule (cubic grids): the three axis operators commute, so
 // the phase that finishes step k can also start step k+1 on the same data layout.
-//   plane phase (units (chain, x)):  [z y]  D  store q  D  [z y]  -> exchange buffer XP
-//   slab phase  (units (chain, y)):  [x]    D  store q  D  [x]    -> exchange buffer XS
+//   plane phase (units (chain, x)):  [z y]  D  store q  D  [y]  -> exchange buffer XP
+//   slab phase  (units (chain, y)):  [z x]  D  store q  D  [x]  -> exchange buffer XS
+// (step k is started with y on planes and finished with z and x on slabs, or started with
+// x on slabs and finished with z and y on planes: three operations per phase, and both
+// phases begin with the row operation A_z)
 // Phase k (k = 0..U) finishes step k-1 (k >= 1) and starts step k (k < U); plane
 // phases have even k.  One exchange per step and no grid barrier: a unit waits only for
 // the release flags of the units whose rows it reads.  The Boltzmann-factor tiles of the
@@ -1069,13 +1072,13 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
         }
         cp_async_commit();
         cp_async_wait_all();
-        if (EO2 && plane && k >= 1) {
+        if (EO2 && k >= 1) {
             static_assert(!EO2 || (TPR == 4 && AxisShapeEO2<N>::GROUPS == 2),
                           "warp w fetches rows 8w..8w+7; row_op_eo2 gives warps 2b, 2b+1 rows 16b..16b+15");
-            // the first operation (A_z along rows) of warps 2b, 2b+1 reads only rows
-            // 16b..16b+15, which these two warps fetched: they start as soon as their own
-            // producers' rows are in, while other rows are still arriving.  A wait that ran
-            // out is caught at the block barrier after the operation.
+            // the first operation of both layouts (A_z along rows) of warps 2b, 2b+1 reads
+            // only rows 16b..16b+15, which these two warps fetched: they start as soon as
+            // their own producers' rows are in, while other rows are still arriving.  A wait
+            // that ran out is caught at the block barrier after the operation.
             asm volatile("bar.sync %0, 64;" ::"r"(1 + (warp >> 1)) : "memory");
         } else {
             __syncthreads();
@@ -1087,9 +1090,10 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
         double* cur = T0;
         double* oth = T1;
         if (k >= 1) {
-            // finish step k-1: the axis ops this layout owns; the last one's epilogue applies
-            // D, writes q(s+1) to the panel staging tile and D q(s+1) to the work tile
-            if (plane) row_z(cur, oth);
+            // finish step k-1: A_z, then the layout's column axis (A_y on planes, A_x on
+            // slabs), whose epilogue applies D, writes q(s+1) to the panel staging tile and
+            // D q(s+1) to the work tile
+            row_z(cur, oth);
             if (warp == 0) bulk_wait_read();  // the previous q store has left QS
             if (!mbar_wait(&s_bar, wpar, a.spin_limit)) s_fail = 1;
             __syncthreads();
@@ -1099,18 +1103,13 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
                 return;
             }
             wpar ^= 1u;
-            ColOut fo{plane ? cur : oth, 0};
+            ColOut fo{cur, 0};
             fo.w0 = W0;
             fo.w1 = W1;
             fo.qs = QS;
             fo.start = k < U;
-            if constexpr (EO2) col_op_eo2<N, N, LF, kFinish>(plane ? oth : cur, fo, sops + (plane ? OFFY : 0));
-            else col_op_ct<N, N, LF, EO, kFinish>(plane ? oth : cur, fo, sops + (plane ? OFFY : 0));
-            if (!plane) {
-                double* tmp = cur;
-                cur = oth;
-                oth = tmp;
-            }
+            if constexpr (EO2) col_op_eo2<N, N, LF, kFinish>(oth, fo, sops + (plane ? OFFY : 0));
+            else col_op_ct<N, N, LF, EO, kFinish>(oth, fo, sops + (plane ? OFFY : 0));
             fence_async_smem();
             __syncthreads();
             if (threadIdx.x == 0) {  // the thread that commits and waits on bulk groups
@@ -1132,16 +1131,10 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
         }
         if (k < U) {
             if (warp == 0) issue_w(k + 1);  // W0/W1 are free: prefetch the next phase's factors
-            // start step k on this layout; the last op's epilogue writes the exchange buffer,
-            // which the other layout finishes next phase
+            // start step k on this layout with its column axis; the epilogue writes the
+            // exchange buffer, which the other layout finishes (A_z, then its own axis) next phase
             const ColOut xo{(plane ? XP : XS) + off, gs};
-            if (plane) {
-                row_z(cur, oth);
-                __syncthreads();
-                col_global(oth, xo, OFFY);
-            } else {
-                col_global(cur, xo, 0);
-            }
+            col_global(cur, xo, plane ? OFFY : 0);
             __syncthreads();
             if (threadIdx.x < N) {  // tell consumer threadIdx.x that tile p of phase k is out
                 __threadfence();

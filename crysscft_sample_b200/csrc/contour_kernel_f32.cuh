@@ -456,20 +456,10 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel_f32(con
         }
         cp_async_commit();
         cp_async_wait_all();
-        // n = 64, even/odd: warp w fetched rows 8w..8w+7 and the plane phase's first
-        // operation (row_op_f32) gives warps 2b, 2b+1 rows 16b..16b+15, so the warp pair
-        // starts as soon as its own producers' rows are in; a wait that ran out is caught
-        // at the block barrier after the operation
-        constexpr bool kPairStart = N == 64 && EO;
-        if (kPairStart && plane && k >= 1) {
-            static_assert(!kPairStart || TPR == 4, "warp w fetches rows 8w..8w+7");
-            asm volatile("bar.sync %0, 64;" ::"r"(1 + (warp >> 1)) : "memory");
-        } else {
-            __syncthreads();
-            if (s_fail) {
-                if (warp == 0) bulk_wait_all();
-                return;
-            }
+        __syncthreads();
+        if (s_fail) {
+            if (warp == 0) bulk_wait_all();
+            return;
         }
         float* cur = T0;
         float* oth = T1;
@@ -479,10 +469,6 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel_f32(con
             if (plane) row_op_f32<N, N, LF, EO>(cur, oth, sops + OFFZ);
             if (warp == 0) bulk_wait_read();  // the previous q store has left QS
             __syncthreads();
-            if (kPairStart && plane && s_fail) {
-                if (warp == 0) bulk_wait_all();
-                return;
-            }
             ColOutF fo{plane ? cur : oth, 0};
             fo.w0 = Wl + blk_of(k - 1) * S::WT;
             fo.w1 = Wl + (k < U ? blk_of(k) : 0) * S::WT;

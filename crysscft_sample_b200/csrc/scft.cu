@@ -102,6 +102,24 @@ int encode_panel_map(CUtensorMap* m, const void* base, int n, long long slots, b
     return SCFT_OK;
 }
 
+// Zero device memory before any of the library's streams uses it.  cudaMemset runs on the
+// legacy default stream and may return before it has run, and the library's streams are
+// non-blocking (they do not wait for the legacy stream), so wait for it here.
+static int zero_device(void* p, size_t bytes) {
+    CK(cudaMemset(p, 0, bytes));
+    CK(cudaStreamSynchronize(0));
+    return SCFT_OK;
+}
+
+// Host-to-device upload for set-up data (operators, tables, task lists).  A cudaMemcpy from
+// pageable host memory may return once the data is staged, before it has reached the
+// device, and the kernels that read it run on non-blocking streams: wait for the copy.
+static int upload(void* dst, const void* src, size_t bytes) {
+    CK(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
+    CK(cudaStreamSynchronize(0));
+    return SCFT_OK;
+}
+
 template <typename T>
 struct DevBuf {
     T* p = nullptr;
@@ -281,8 +299,8 @@ int upload_fft_tables(OpsSet& s, int axis, int nf, int ext, long double L, long 
     }
     CKR(s.d_fft_g[axis].alloc((size_t)nf));
     CKR(s.d_fft_tw[axis].alloc((size_t)nf));
-    CK(cudaMemcpy(s.d_fft_g[axis].p, g.data(), g.size() * sizeof(double), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(s.d_fft_tw[axis].p, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    CKR(upload(s.d_fft_g[axis].p, g.data(), g.size() * sizeof(double)));
+    CKR(upload(s.d_fft_tw[axis].p, tw.data(), tw.size() * sizeof(double2)));
     std::vector<float> gf((size_t)nf);
     std::vector<float2> twf((size_t)nf);
     for (int k = 0; k < nf; ++k) {
@@ -291,8 +309,8 @@ int upload_fft_tables(OpsSet& s, int axis, int nf, int ext, long double L, long 
     }
     CKR(s.f_fft_g[axis].alloc((size_t)nf));
     CKR(s.f_fft_tw[axis].alloc((size_t)nf));
-    CK(cudaMemcpy(s.f_fft_g[axis].p, gf.data(), gf.size() * sizeof(float), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(s.f_fft_tw[axis].p, twf.data(), twf.size() * sizeof(float2), cudaMemcpyHostToDevice));
+    CKR(upload(s.f_fft_g[axis].p, gf.data(), gf.size() * sizeof(float)));
+    CKR(upload(s.f_fft_tw[axis].p, twf.data(), twf.size() * sizeof(float2)));
     s.fft_nf[axis] = nf;
     s.fft_ext[axis] = ext;
     return SCFT_OK;
@@ -422,10 +440,10 @@ int upload_operator(const std::vector<long double>& A, int n, OpsSet& s, int axi
     CKR(s.d_opT[axis].alloc(nn));
     CKR(s.f_op[axis].alloc(nn));
     CKR(s.f_opT[axis].alloc(nn));
-    CK(cudaMemcpy(s.d_op[axis].p, d.data(), nn * sizeof(double), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(s.d_opT[axis].p, dt.data(), nn * sizeof(double), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(s.f_op[axis].p, f.data(), nn * sizeof(float), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(s.f_opT[axis].p, ft.data(), nn * sizeof(float), cudaMemcpyHostToDevice));
+    CKR(upload(s.d_op[axis].p, d.data(), nn * sizeof(double)));
+    CKR(upload(s.d_opT[axis].p, dt.data(), nn * sizeof(double)));
+    CKR(upload(s.f_op[axis].p, f.data(), nn * sizeof(float)));
+    CKR(upload(s.f_opT[axis].p, ft.data(), nn * sizeof(float)));
     return SCFT_OK;
 }
 
@@ -775,19 +793,15 @@ struct scft_solver_s {
         s->eo2 = eo2_axes == 3;
         if (s->eo2) {
             CKR(s->d_packed2.alloc(s->h_packed2.size()));
-            CK(cudaMemcpy(s->d_packed2.p, s->h_packed2.data(), s->h_packed2.size() * sizeof(double),
-                          cudaMemcpyHostToDevice));
+            CKR(upload(s->d_packed2.p, s->h_packed2.data(), s->h_packed2.size() * sizeof(double)));
         }
         CKR(s->d_packed.alloc(s->h_packed.size()));
-        CK(cudaMemcpy(s->d_packed.p, s->h_packed.data(), s->h_packed.size() * sizeof(double),
-                      cudaMemcpyHostToDevice));
+        CKR(upload(s->d_packed.p, s->h_packed.data(), s->h_packed.size() * sizeof(double)));
         CKR(s->f_packed.alloc(s->h_packed_f32.size()));
-        CK(cudaMemcpy(s->f_packed.p, s->h_packed_f32.data(), s->h_packed_f32.size() * sizeof(float),
-                      cudaMemcpyHostToDevice));
+        CKR(upload(s->f_packed.p, s->h_packed_f32.data(), s->h_packed_f32.size() * sizeof(float)));
         if (s->h16_axes == 3) {
             CKR(s->h16_packed.alloc(s->h_packed_h16.size()));
-            CK(cudaMemcpy(s->h16_packed.p, s->h_packed_h16.data(), s->h_packed_h16.size() * sizeof(uint16_t),
-                          cudaMemcpyHostToDevice));
+            CKR(upload(s->h16_packed.p, s->h_packed_h16.data(), s->h_packed_h16.size() * sizeof(uint16_t)));
         }
         ops = s.get();
         ops_cache[ds_] = std::move(s);
@@ -821,8 +835,8 @@ struct scft_solver_s {
                 OpsSet* o = ops->term(t);
                 CKR(o->d_dop[ax].alloc((size_t)n * n));
                 CKR(o->d_dopT[ax].alloc((size_t)n * n));
-                CK(cudaMemcpy(o->d_dop[ax].p, d.data(), d.size() * sizeof(double), cudaMemcpyHostToDevice));
-                CK(cudaMemcpy(o->d_dopT[ax].p, dt.data(), dt.size() * sizeof(double), cudaMemcpyHostToDevice));
+                CKR(upload(o->d_dop[ax].p, d.data(), d.size() * sizeof(double)));
+                CKR(upload(o->d_dopT[ax].p, dt.data(), dt.size() * sizeof(double)));
             }
         }
         ops->have_dop = true;
@@ -1070,7 +1084,7 @@ struct scft_diblock_s {
         if (nclusters < 2) return SCFT_OK;
         if (!ctrl.p) {
             CKR(ctrl.alloc(2));
-            CK(cudaMemset(ctrl.p, 0, 2 * sizeof(unsigned)));
+            CKR(zero_device(ctrl.p, 2 * sizeof(unsigned)));
         }
         cluster_f32 = true;
         persistent = true;
@@ -1140,7 +1154,7 @@ struct scft_diblock_s {
         if (flags.n != (size_t)(4 * nx * nx)) CKR(flags.alloc((size_t)4 * nx * nx));
         if (!ctrl.p) {
             CKR(ctrl.alloc(2));
-            CK(cudaMemset(ctrl.p, 0, 2 * sizeof(unsigned)));
+            CKR(zero_device(ctrl.p, 2 * sizeof(unsigned)));
         }
         alternating = true;
         persistent = true;
@@ -1235,7 +1249,7 @@ struct scft_diblock_s {
         persistent_smem = smem;
         if (!ctrl.p) {
             CKR(ctrl.alloc(2));
-            CK(cudaMemset(ctrl.p, 0, 2 * sizeof(unsigned)));
+            CKR(zero_device(ctrl.p, 2 * sizeof(unsigned)));
         }
         persistent = true;
         return SCFT_OK;
@@ -1775,9 +1789,9 @@ int scft_diblock_create(scft_solver_t s, double fA, double ds, double xN, double
     CKR(d->partials.alloc(5 * kRedMaxBlocks));
     CKR(d->hist.alloc((size_t)d->hist_cap * HIST_STRIDE));
     CKR(d->state.alloc(1));
-    CK(cudaMemset(d->state.p, 0, sizeof(IterState)));
-    CK(cudaMemset(d->phiA.p, 0, M * sizeof(double)));
-    CK(cudaMemset(d->phiB.p, 0, M * sizeof(double)));
+    CKR(zero_device(d->state.p, sizeof(IterState)));
+    CKR(zero_device(d->phiA.p, M * sizeof(double)));
+    CKR(zero_device(d->phiB.p, M * sizeof(double)));
     CKR(diblock_buffers(d.get(), d->precision));
     ++s->users;  // the solver outlives this context (scft_solver_destroy defers)
     *out = d.release();
@@ -2446,9 +2460,9 @@ struct scft_batch_s {
         CKR(team_chains.alloc(hc.size()));
         CKR(team_tasks.alloc(tasks.size()));
         CKR(team_begin.alloc(begin.size()));
-        CK(cudaMemcpy(team_chains.p, hc.data(), hc.size() * sizeof(TeamChain), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(team_tasks.p, tasks.data(), tasks.size() * sizeof(TeamTask), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(team_begin.p, begin.data(), begin.size() * sizeof(int), cudaMemcpyHostToDevice));
+        CKR(upload(team_chains.p, hc.data(), hc.size() * sizeof(TeamChain)));
+        CKR(upload(team_tasks.p, tasks.data(), tasks.size() * sizeof(TeamTask)));
+        CKR(upload(team_begin.p, begin.data(), begin.size() * sizeof(int)));
         team_grid = G;
         team_smem = smem;
         team_ntasks = tasks.size();
@@ -2593,11 +2607,18 @@ struct scft_batch_s {
             // are not a numeric failure), every instance's word read and cleared
             {
                 int first = SCFT_OK;
+                std::string what;
                 for (size_t i = 0; i < n; ++i) {
                     const int r = diblock_check_device_error(runs[i], main);
-                    if (first == SCFT_OK) first = r;
+                    if (first == SCFT_OK && r != SCFT_OK) {
+                        first = r;
+                        what = "instance " + std::to_string(i) + " (grid " +
+                               std::to_string(runs[i]->solver->grid_phy[0]) + ", batch form " + std::to_string(form) +
+                               (i < in_team.size() && in_team[i] ? ", in the one launch" : ", own kernels") + "): " +
+                               g_last_error;
+                    }
                 }
-                if (first != SCFT_OK) return first;
+                if (first != SCFT_OK) return fail(first, what);
             }
             for (size_t i = 0; i < n; ++i) {
                 scft_diblock_t d = runs[i];
