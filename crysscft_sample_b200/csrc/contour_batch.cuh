@@ -15,11 +15,12 @@
 // contour_alt_kernel (same tile operations and epilogues, in the same order), so the
 // results are bit-identical to the per-instance kernel.
 //
-// Scheduling: the host gives every CTA an ordered task list (chain, rank, team size).
-// Teams share CTAs only in one global order (tasks sorted by planned start time, ties by
-// chain index), so the earliest unfinished task always has all its members at it and the
-// launch cannot deadlock.  Every wait is bounded; a CTA that gives up sets the batch's
-// abort word, which every other wait polls, drains its own bulk copies and leaves.
+// Scheduling: the host (team_schedule in scft.cu) gives every CTA an ordered task list
+// (chain, rank, team size).  CTAs are grouped in columns of one team size; every CTA of a
+// column runs the same chains in the same order, so a team never waits for a member busy
+// with another task and the launch cannot deadlock.  Every wait is bounded; a CTA that
+// gives up sets the batch's abort word, which every other wait polls, drains its own bulk
+// copies and leaves.
 #pragma once
 
 namespace crysscft {
