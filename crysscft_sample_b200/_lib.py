@@ -81,6 +81,7 @@ SIGNATURES = {
     "scft_diblock_set_mixing": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double]),
     "scft_diblock_get_residuals": (ctypes.c_int, [_vp, _dp, _sz, _szp]),
     "scft_diblock_set_wait_limit": (ctypes.c_int, [_vp, ctypes.c_longlong]),
+    "scft_diblock_set_phi_form": (ctypes.c_int, [_vp, ctypes.c_int]),
 }
 
 _lib = None

@@ -67,6 +67,11 @@ struct ContourArgs {
     int* error;             // bit 0: barrier wait gave up
     long long spin_limit;
     unsigned* flags;        // alternating kernel: [chain][plane|slab][consumer][producer] last finished phase + 1, zeroed by the host
+    // alternating kernel, fused phi (null: off): sums of q(s) q+(s) per chain, block A|B,
+    // layout plane|slab and tile, in panel order ([chain][block][layout][tile][N * N]), and
+    // per chain and unit: U/2 once the q stores of phases < U/2 have landed (zeroed by the host)
+    double* phi_acc;
+    unsigned* done;
     // alternating kernel: Boltzmann and staging tiles in 8-column panels ([z / 8][row][z % 8],
     // rows y in plane tiles, x in slab tiles), [0] plane and [1] slab view; contour store of
     // each chain as (z % 8, row, z / 8, tile, slot), Boltzmann factors of blocks A and B
@@ -877,6 +882,31 @@ __device__ __forceinline__ void tma_store_5d(const CUtensorMap* map, const void*
                  ::"l"(map), "r"(smem_u32(src)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4)
                  : "memory");
 }
+// tiled TMA: the 5-D box at (c0, .., c4) into shared memory, completing on `bar`
+__device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3, int c4,
+                                            unsigned long long* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], [%7];"
+        ::"r"(smem_u32(dst)), "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(bar))
+        : "memory");
+}
+// the 5-D box at (c0, .., c4) of a tensor map into L2 (no shared memory, no completion)
+__device__ __forceinline__ void tma_prefetch_l2_5d(const CUtensorMap* map, int c0, int c1, int c2, int c3, int c4) {
+    asm volatile("cp.async.bulk.prefetch.tensor.5d.L2.global.tile [%0, {%1, %2, %3, %4, %5}];"
+                 ::"l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4)
+                 : "memory");
+}
+// every bulk group of this thread but the newest one (three) has completed (writes performed)
+__device__ __forceinline__ void bulk_wait_but_newest() { asm volatile("cp.async.bulk.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_newest3() { asm volatile("cp.async.bulk.wait_group 3;" ::: "memory"); }
+// orders this thread's generic-proxy accesses of global memory with its bulk copies
+__device__ __forceinline__ void fence_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
+// bulk reduction: dst[i] += src[i] for `bytes` / 8 doubles, shared to global, tracked by bulk groups
+__device__ __forceinline__ void bulk_reduce_add_f64(double* dst, const void* src, unsigned bytes) {
+    asm volatile("cp.reduce.async.bulk.global.shared::cta.bulk_group.add.f64 [%0], [%1], %2;"
+                 ::"l"(dst), "r"(smem_u32(src)), "r"(bytes)
+                 : "memory");
+}
 // N x N tile from global (row stride gs) into shared memory (row stride LF) with cp.async
 template <int N, int LF>
 __device__ __forceinline__ void tile_fetch(double* sm, const double* gm, long long gs) {
@@ -960,6 +990,7 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
     double* W1 = W0 + S::WT;    // D of the step being started
     double* QS = W1 + S::WT;    // finished q(s+1), drained by bulk stores
     __shared__ __align__(8) unsigned long long s_bar;  // completion of the W0/W1 bulk loads
+    __shared__ __align__(8) unsigned long long s_xbar; // fused phi: the other chain's slot tile
     __shared__ int s_fail;
 
     constexpr long long M = (long long)N * N * N;
@@ -972,9 +1003,11 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
     }
     if (u >= units) return;
     const int warp = threadIdx.x >> 5;
+    const bool fphi = a.phi_acc != nullptr;  // the host sets it only for two chains
     {
-        const void* tiles[3] = {W0, W1, QS};
-        const int e = tma_alignment_error(tiles, 3, &a.tm_pq[0][0], 4) | tma_alignment_error(tiles, 0, &a.tm_pw[0][0], 4);
+        const void* tiles[4] = {W0, W1, QS, T1};
+        const int e = tma_alignment_error(tiles, fphi ? 4 : 3, &a.tm_pq[0][0], 4) |
+                      tma_alignment_error(tiles, 0, &a.tm_pw[0][0], 4);
         if (e) {
             if (threadIdx.x == 0) atomicOr(a.error, e);
             return;
@@ -985,6 +1018,7 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
     if (threadIdx.x == 0) {
         s_fail = 0;
         mbar_init(&s_bar, 1);
+        mbar_init(&s_xbar, 1);
         fence_mbar_init();
     }
     __syncthreads();
@@ -993,6 +1027,29 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
     const int c = u >= N ? 1 : 0, p = u - c * N;
     const int dir = c ? a.dir[1] : a.dir[0];
     const long long slot0 = c ? a.slot0[1] : a.slot0[0];
+    // Fused phi.  The phase that finishes slot s of this chain sums q(s) q+(s) over the
+    // unit's tile when the other chain finished slot s at least two phases earlier (the
+    // second half of the contour: chain 0 the slots above U/2, chain 1 those below).  The
+    // other chain's tile of slot s is bulk-loaded into T1 (free between the finishing
+    // operation and the next phase's A_z); after this phase's release the products replace
+    // q(s) in QS (its store has read it) and one bulk add (cp.reduce.async.bulk) puts them
+    // into the unit's accumulator tile of the slot's block and the layout.  Per-element
+    // atomics were measured slower: 4096 FP64 L2 atomics per unit and phase slowed the
+    // exchange more than the separate phi pass costs.  A tile's bulk adds are issued only
+    // after the previous one has completed, so the sums run in phase order (deterministic).
+    // The host enables this only for chain 0 forward from slot 0 and chain 1 backward from
+    // slot U, U even: then kp = U - k, and the slots read are those stored before U/2.
+    // Slots 0, NsA (trapezoid weights), U/2 (both chains finish it in the same phase) and
+    // U are left to the finishing kernel.
+    const int co = 1 - c;
+    double* acc_unit = fphi ? a.phi_acc + (size_t)c * 4 * M + (size_t)p * PLANE : nullptr;
+    auto x_active = [&](int k) -> bool {
+        const long long s = slot0 + (long long)dir * k, kq = (s - a.slot0[co]) * a.dir[co];
+        return fphi && k >= 1 && k <= U && kq >= 1 && kq <= k - 2 && ((k - kq) & 1) == 0 && s != a.NsA;
+    };
+    unsigned xpar = 0;   // parity of the pending phase of s_xbar
+    unsigned x_seen = 0; // thread 0: the other unit's landed-store count last acquired
+    bool x_pend = false; // this thread gave up waiting for an issued slot-tile load
     double* q = c ? a.q[1] : a.q[0];
     double* XP = c ? a.xbuf[1] : a.xbuf[0];  // written by plane phases
     double* XS = XP + M;                     // written by slab phases
@@ -1023,6 +1080,7 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
     // error exit: let this block's bulk copies finish (bounded), then return
     auto drain = [&](bool w_pending) {
         if (w_pending) mbar_wait(&s_bar, wpar, kDrainSpins);
+        if (x_pend) mbar_wait(&s_xbar, xpar, kDrainSpins);
         if (warp == 0) bulk_wait_all();
     };
 
@@ -1045,6 +1103,11 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
         const bool plane = (k & 1) == 0;
         const long long off = plane ? (long long)p * PLANE : (long long)p * N;
         const long long gs = plane ? N : PLANE;
+        // fused phi: slot finished in this phase, and the phase kp in which the other chain
+        // finished (stored) the same slot on the same layout and tile
+        const long long s_fin = slot0 + (long long)dir * k;
+        const long long kp = (s_fin - a.slot0[co]) * a.dir[co];
+        const bool xact = x_active(k);
         if (k == 0) {
             tile_fetch<N, LF>(T0, q + slot0 * M + off, gs);
         } else {
@@ -1115,6 +1178,33 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
             if (threadIdx.x == 0) {  // the thread that commits and waits on bulk groups
                 tma_store_5d(&a.tm_pq[c][plane ? 0 : 1], QS, 0, 0, 0, p, (int)(slot0 + (long long)dir * k));
                 bulk_commit();
+                if (fphi) {
+                    if (xact) {  // T1 was last read by the finishing operation (fenced above)
+                        // the other unit releases once; after the first acquire that saw it, no
+                        // further round trip to L2 on warp 0's way to the phase's last operation
+                        const unsigned* df = a.done + (size_t)co * N + p;
+                        long long spins = 0;
+                        while (x_seen < (unsigned)(kp + 1)) {
+                            x_seen = ld_acquire_u32(df);
+                            if (x_seen >= (unsigned)(kp + 1)) break;
+                            if (++spins > a.spin_limit) break;
+                            if (spins > 64) __nanosleep(32);
+                        }
+                        if (spins > a.spin_limit) {
+                            atomicOr(a.error, 32);
+                            s_fail = 1;  // no load issued; the block leaves after the next barrier
+                        } else {
+                            fence_async_global();
+                            mbar_expect_tx(&s_xbar, TILE_BYTES);
+                            tma_load_5d(T1, &a.tm_pq[co][plane ? 0 : 1], 0, 0, 0, p, (int)s_fin, &s_xbar);
+                        }
+                    }
+                    // the next phase's tile into L2 now (the old slots are in HBM); it was
+                    // stored at least three phases ago, and L2 is coherent with that store
+                    if (x_active(k + 1))
+                        tma_prefetch_l2_5d(&a.tm_pq[co][plane ? 1 : 0], 0, 0, 0, p, (int)(s_fin + dir));
+
+                }
             }
         }
         if (k == 0) {
@@ -1136,12 +1226,71 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
             const ColOut xo{(plane ? XP : XS) + off, gs};
             col_global(cur, xo, plane ? OFFY : 0);
             __syncthreads();
+            if (xact && s_fail) {  // thread 0 gave up on the other chain's store: no load in flight
+                drain(true);
+                return;
+            }
             if (threadIdx.x < N) {  // tell consumer threadIdx.x that tile p of phase k is out
                 __threadfence();
                 st_release_u32((plane ? fl_plane : fl_slab) + (size_t)threadIdx.x * N + p, (unsigned)(k + 1));
             }
+            if (fphi && threadIdx.x == 0 && 2 * k == U) {
+                // the other chain reads only slots this chain stored before the midpoint
+                // phase (kp <= U/2 - 1 above): one release, once those stores have landed
+                // (every bulk group but this phase's q store has completed).  A release in
+                // every phase, right after the q store was issued, cost 0.15 ms per iteration.
+                bulk_wait_but_newest();
+                fence_async_global();
+                st_release_u32(a.done + (size_t)c * N + p, (unsigned)k);
+            }
         }
-        __syncthreads();
+        if (fphi && k == 0) {  // zero the accumulator tiles, long before the first bulk add
+            for (int t4 = 0; t4 < 4; ++t4)
+                for (int i = threadIdx.x; i < N * N; i += kContourThreads) acc_unit[(size_t)t4 * M + i] = 0.0;
+            fence_async_global();
+        }
+        if (xact) {  // fused phi: QS holds q(s) of this chain, T1 the other chain's, same panels
+            if (threadIdx.x == 0) bulk_wait_read();  // the q(s) store has read QS
+            if (mbar_wait(&s_xbar, xpar, a.spin_limit)) {
+                xpar ^= 1u;
+            } else {
+                x_pend = true;
+                s_fail = 1;
+                atomicOr(a.error, 2);
+            }
+            __syncthreads();
+            if (s_fail) {
+                drain(k < U);
+                return;
+            }
+            // QS <- q(s) q+(s), then one bulk add into the accumulator tile; the next phase's
+            // wait for QS to be read (before its finishing operation) covers it.  The barrier
+            // after the products also ends the phase.
+            for (int i = 2 * threadIdx.x; i < N * N; i += 2 * kContourThreads) {
+                double2 v = *reinterpret_cast<double2*>(QS + i);
+                const double2 w = *reinterpret_cast<const double2*>(T1 + i);
+                v.x *= w.x;
+                v.y *= w.y;
+                *reinterpret_cast<double2*>(QS + i) = v;
+            }
+            fence_async_smem();
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                // the add of two phases back (same layout, possibly the same tile) has
+                // completed: at most this phase's store and the last phase's store and add
+                // are pending, so the adds into one tile apply in phase order
+                bulk_wait_newest3();
+                bulk_reduce_add_f64(acc_unit + (size_t)((s_fin < a.NsA ? 0 : 2) + (plane ? 0 : 1)) * M, QS,
+                                    TILE_BYTES);
+                bulk_commit();
+            }
+        } else {
+            __syncthreads();
+            if (fphi && s_fail) {
+                drain(k < U);
+                return;
+            }
+        }
     }
     if (warp == 0) bulk_wait_all();
 }

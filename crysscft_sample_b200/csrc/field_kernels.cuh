@@ -189,6 +189,48 @@ __global__ void phi_kernel(const T* __restrict__ q, const T* __restrict__ qc, do
     }
 }
 
+// phi from the alternating contour kernel's fused sums (cubic grid n^3, U = NsA + NsB even).
+// acc[c][block][layout][tile][panel element] holds, for chain c, the sum of q(s) q+(s) over
+// the slots s of the block that the chain finished in that layout, except slots 0, NsA,
+// U/2 and U; those are added here with the trapezoid weights of integrate_phi
+// (src/crysSCFT_sample.cpp:348-360: 1/2 at both ends of each block, 1 inside).  The panel
+// element of grid point (x, y, z) is (z / 8) * 8n + row * 8 + z % 8, with row y in plane
+// tile x and row x in slab tile y.
+__global__ void phi_fused_finish_kernel(const double* __restrict__ acc, const double* __restrict__ q,
+                                        const double* __restrict__ qc, double* __restrict__ phiA,
+                                        double* __restrict__ phiB, const IterState* st, double fA, long long NsA,
+                                        long long NsB, int n) {
+    const long long n2 = (long long)n * n, M = n2 * n, U = NsA + NsB;
+    const double Q = st->Q;
+    const double cA = fA / (NsA * Q), cB = (1 - fA) / (NsB * Q);
+    long long sp[4] = {0, NsA, U / 2, U};
+    int nsp = 4;
+    if (U / 2 == NsA) {  // the midpoint is the block boundary
+        sp[2] = U;
+        nsp = 3;
+    }
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < M; i += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(i / n2), y = (int)((i / n) % n), z = (int)(i % n);
+        const long long zp = (long long)(z >> 3) * 8 * n + (z & 7);
+        const long long ep = x * n2 + zp + y * 8;  // plane tile x, row y
+        const long long es = y * n2 + zp + x * 8;  // slab tile y, row x
+        double a = 0.0, b = 0.0;
+        for (int c = 0; c < 2; ++c) {
+            const double* t = acc + (size_t)c * 4 * M;
+            a += t[ep] + t[M + es];
+            b += t[2 * M + ep] + t[3 * M + es];
+        }
+        for (int j = 0; j < nsp; ++j) {
+            const long long s = sp[j];
+            const double w = q[s * M + i] * qc[s * M + i];
+            if (s <= NsA) a += (s == 0 || s == NsA ? 0.5 : 1.0) * w;
+            if (s >= NsA) b += (s == NsA || s == U ? 0.5 : 1.0) * w;
+        }
+        phiA[i] = cA * a;
+        phiB[i] = cB * b;
+    }
+}
+
 __global__ void __launch_bounds__(kRedThreads)
 energy_kernel(const double* __restrict__ wA, const double* __restrict__ wB,
               const double* __restrict__ phiA, const double* __restrict__ phiB,

@@ -102,6 +102,10 @@ int encode_panel_map(CUtensorMap* m, const void* base, int n, long long slots, b
     return SCFT_OK;
 }
 
+// Flags of the alternating kernels at n^3: [chain][plane|slab][consumer][producer] exchange
+// flags, then [chain][unit] landed-store counts of the fused phi sums.
+static size_t alt_flag_count(int nx) { return (size_t)4 * nx * nx + (size_t)2 * nx; }
+
 // Zero device memory before any of the library's streams uses it.  cudaMemset runs on the
 // legacy default stream and may return before it has run, and the library's streams are
 // non-blocking (they do not wait for the legacy stream), so wait for it here.
@@ -1026,6 +1030,9 @@ struct scft_diblock_s {
     int last_form = 0;                    // force_form the current launch plan was built with
     DevBuf<double> d_xch;                 // exchange buffers, 2 x space_size_phy per chain
     DevBuf<unsigned> flags;               // per-unit phase flags of the alternating kernel
+    bool fused_phi = true;                // FP64 alternating kernel sums phi itself (scft_diblock_set_phi_form)
+    bool phi_fused = false;               // the last launch_contour ran with the fused phi sums
+    DevBuf<double> phi_acc;               // its sums: [chain][block][layout][tile][n^2], 8 x space_size_phy
     int last_iter_precision = -1;         // precision of the iteration whose contour is stored
     DevBuf<double> stress_buf;            // batched temporaries of scft_diblock_stress
     ContourFnF contour_fn_f32 = nullptr;  // FP32 (3xTF32) contour kernel
@@ -1151,7 +1158,7 @@ struct scft_diblock_s {
         persistent_grid = 2 * nx;
         persistent_smem = smem;
         if (!f_xch.p) CKR(f_xch.alloc(4 * M));
-        if (flags.n != (size_t)(4 * nx * nx)) CKR(flags.alloc((size_t)4 * nx * nx));
+        if (flags.n != alt_flag_count(nx)) CKR(flags.alloc(alt_flag_count(nx)));
         if (!ctrl.p) {
             CKR(ctrl.alloc(2));
             CKR(zero_device(ctrl.p, 2 * sizeof(unsigned)));
@@ -1238,7 +1245,7 @@ struct scft_diblock_s {
             }
         }
         if (!d_xch.p) CKR(d_xch.alloc(4 * M));
-        if (alternating && flags.n != (size_t)(4 * nx * nx)) CKR(flags.alloc((size_t)4 * nx * nx));
+        if (alternating && flags.n != alt_flag_count(nx)) CKR(flags.alloc(alt_flag_count(nx)));
         CK(cudaFuncSetAttribute(contour_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 0;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, contour_fn, kContourThreads, smem));
@@ -1286,6 +1293,14 @@ struct scft_diblock_s {
         a.spin_limit = spin_limit;
         a.flags = flags.p;
         CK(cudaMemsetAsync(ctrl.p, 0, sizeof(unsigned), st));
+        // phi summed inside the alternating kernel: both chains, U even (the slots the two
+        // chains finish meet on the same layout), both blocks non-empty
+        phi_fused = alternating && fused_phi && U % 2 == 0 && NsA >= 1 && NsB >= 1;
+        if (phi_fused) {
+            if (phi_acc.n != 8 * M) CKR(phi_acc.alloc(8 * M));
+            a.phi_acc = phi_acc.p;
+            a.done = flags.p + 4 * solver->grid_phy[0] * solver->grid_phy[0];
+        }
         if (alternating) {
             const int n = (int)solver->grid_phy[0];
             for (int v = 0; v < 2; ++v) {  // panel tiles, plane [0] and slab [1] views
@@ -1319,6 +1334,7 @@ struct scft_diblock_s {
         const long long MM = (long long)M;
         const int blocks = grid_blocks(MM, 256);
         size_t launches = 0;
+        bool fused = false;  // phi was summed by this iteration's contour kernel
         if (parts & kPartPrep) {
             prep_kernel<T><<<blocks, 256, 0, st>>>(wA.p, wB.p, ksi.p, wAds, wBds, q, qc + U * M, xN, ds, MM);
             CK(cudaGetLastError());
@@ -1328,8 +1344,12 @@ struct scft_diblock_s {
             if (phase_events) CK(cudaEventRecord(phase_events[1], st));
             const size_t before = solver->launches;
             if (persistent) {
-                if constexpr (sizeof(T) == 8) CKR(launch_contour(st, wAds, wBds, q, qc));
-                else CKR(launch_contour_f32(st, wAds, wBds, q, qc));
+                if constexpr (sizeof(T) == 8) {
+                    CKR(launch_contour(st, wAds, wBds, q, qc));
+                    fused = phi_fused;
+                } else {
+                    CKR(launch_contour_f32(st, wAds, wBds, q, qc));
+                }
                 ++solver->launches;
             }
             for (size_t t_ = 0; t_ < U && !persistent; ++t_) {
@@ -1355,8 +1375,15 @@ struct scft_diblock_s {
         const int rblocks = (int)std::min<long long>(kRedMaxBlocks, (MM + kRedThreads - 1) / kRedThreads);
         q_reduce_kernel<T><<<rblocks, kRedThreads, 0, st>>>(qc, MM, partials.p, state.p);
         CK(cudaGetLastError());
-        phi_kernel<T><<<grid_blocks((MM + 1) / 2, 256), 256, 0, st>>>(q, qc, phiA.p, phiB.p, state.p, fA, (long long)NsA,
-                                              (long long)NsB, MM);
+        if constexpr (sizeof(T) == 8) {
+            if (fused)
+                phi_fused_finish_kernel<<<grid_blocks(MM, 256), 256, 0, st>>>(
+                    phi_acc.p, q, qc, phiA.p, phiB.p, state.p, fA, (long long)NsA, (long long)NsB,
+                    (int)solver->grid_phy[0]);
+        }
+        if (!fused)
+            phi_kernel<T><<<grid_blocks((MM + 1) / 2, 256), 256, 0, st>>>(q, qc, phiA.p, phiB.p, state.p, fA,
+                                                                          (long long)NsA, (long long)NsB, MM);
         CK(cudaGetLastError());
         if (phase_events) CK(cudaEventRecord(phase_events[3], st));
         energy_kernel<<<rblocks, kRedThreads, 0, st>>>(wA.p, wB.p, phiA.p, phiB.p, ksi.p, xN, MM,
@@ -1875,6 +1902,20 @@ int scft_diblock_set_wait_limit(scft_diblock_t d, long long spins) {
         d->captured_gen = ~0ULL;
         d->saved_gen[0] = d->saved_gen[1] = ~0ULL;
         d->spin_limit = spins;
+    }
+    return SCFT_OK;
+}
+
+int scft_diblock_set_phi_form(scft_diblock_t d, int fused) {
+    if (!d) return fail(SCFT_ERR_INVALID_ARG, "null handle");
+    if (fused != 0 && fused != 1) return fail(SCFT_ERR_INVALID_ARG, "phi form: 1 fused, 0 separate pass");
+    CK(cudaSetDevice(d->solver->device));
+    CK(cudaStreamSynchronize(d->solver->stream));
+    if ((fused != 0) != d->fused_phi) {
+        // the phi kernel is part of the captured FP64 iteration graph
+        d->captured_gen = ~0ULL;
+        d->saved_gen[0] = d->saved_gen[1] = ~0ULL;
+        d->fused_phi = fused != 0;
     }
     return SCFT_OK;
 }

@@ -164,6 +164,11 @@ class DiblockSCFT:
         """Poll limit of the contour kernels' bounded waits (see scft_diblock_set_wait_limit)."""
         check(_lib.load().scft_diblock_set_wait_limit(self._h, int(spins)))
 
+    def set_phi_form(self, fused: bool = True):
+        """Integrate phi inside the whole-contour kernel (True, the default) or in a separate
+        pass over the stored contour (False); see scft_diblock_set_phi_form."""
+        check(_lib.load().scft_diblock_set_phi_form(self._h, 1 if fused else 0))
+
     def residuals(self) -> np.ndarray:
         """rms residual sqrt(<r, r> / 2M) of each iteration of the last iterate() call."""
         n = ctypes.c_size_t()

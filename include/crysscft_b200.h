@@ -216,6 +216,16 @@ int scft_diblock_set_mixing(scft_diblock_t d, int history, double beta);
  * (it has no device code); a small limit is how the timeout path is tested. */
 int scft_diblock_set_wait_limit(scft_diblock_t d, long long spins);
 
+/* Where the FP64 iterations integrate phi_A and phi_B over the contour (integrate_phi,
+ * src/crysSCFT_sample.cpp:348-360, trapezoid weights): fused = 1 (default) lets the
+ * whole-contour kernel on cubic grids add q(s) q+(s) tile by tile as the second chain
+ * reaches each slot, so a short kernel finishes phi instead of a pass over the stored
+ * contour; fused = 0 always uses that separate pass.  The two agree to rounding (the sums
+ * run in a different order).  The fused form applies to the alternating whole-contour
+ * kernel with an even number of contour steps; other plans use the separate pass either
+ * way.  No counterpart in the reference (a form switch of this library). */
+int scft_diblock_set_phi_form(scft_diblock_t d, int fused);
+
 /* rms residual sqrt(<r, r> / 2M) of each iteration of the last scft_diblock_iterate
  * call (any mixing); *count = number of iterations, at most `capacity` copied. */
 int scft_diblock_get_residuals(scft_diblock_t d, double* out, size_t capacity, size_t* count);
