@@ -320,6 +320,8 @@ struct AltShapeF {
     static constexpr int WT = N * N;
     // + 128: the carve-up starts at the first 128-byte boundary of the dynamic window
     static constexpr size_t SMEM = (size_t)(OPS_PAD + 2 * TILE + 5 * WT) * sizeof(float) + 128;
+    // with the fused phi sums: the other chain's tile (FP32) and the products (FP64)
+    static constexpr size_t SMEM_FUSED = SMEM + (size_t)WT * (sizeof(float) + sizeof(double));
 };
 
 struct ContourArgsF {
@@ -335,6 +337,8 @@ struct ContourArgsF {
     int* error;
     long long spin_limit;
     unsigned* flags;       // [chain][plane|slab][consumer][producer], zeroed by the host
+    double* phi_acc;       // fused phi sums (null: off; the launch then has SMEM_FUSED), as ContourArgs
+    unsigned* done;
     alignas(64) CUtensorMap tm_pq[2][2];  // panel tiles, as ContourArgs::tm_pq / tm_pw
     alignas(64) CUtensorMap tm_pw[2][2];
 };
@@ -358,7 +362,10 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel_f32(con
     float* WP = T1 + S::TILE;  // [block A, block B] plane-layout factors of this unit
     float* WS = WP + 2 * S::WT;  // [block A, block B] slab-layout factors
     float* QS = WS + 2 * S::WT;  // finished q(s+1), drained by bulk stores
+    float* XF = QS + S::WT;      // fused phi: the other chain's tile of the slot
+    double* PD = reinterpret_cast<double*>(XF + S::WT);  // fused phi: the products, bulk-added
     __shared__ __align__(8) unsigned long long s_bar;
+    __shared__ __align__(8) unsigned long long s_xbar;
     __shared__ int s_fail;
 
     constexpr long long M = (long long)N * N * N;
@@ -383,18 +390,33 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel_f32(con
     unsigned* fl_plane = a.flags + (size_t)c * 2 * N * N;  // written by plane units
     unsigned* fl_slab = fl_plane + (size_t)N * N;           // written by slab units
     const int U = a.t_end;
+    const bool fphi = a.phi_acc != nullptr;
     {
-        const void* tiles[6] = {WP, WP + S::WT, WS, WS + S::WT, QS, T0};
-        const int e = tma_alignment_error(tiles, 5, &a.tm_pq[0][0], 4) | tma_alignment_error(tiles, 0, &a.tm_pw[0][0], 4);
+        const void* tiles[7] = {WP, WP + S::WT, WS, WS + S::WT, QS, XF, PD};
+        const int e = tma_alignment_error(tiles, fphi ? 7 : 5, &a.tm_pq[0][0], 4) |
+                      tma_alignment_error(tiles, 0, &a.tm_pw[0][0], 4);
         if (e) {
             if (threadIdx.x == 0) atomicOr(a.error, e);
             return;
         }
     }
+    // Fused phi, as in the FP64 alternating kernel (contour_kernel.cuh): in the second half of
+    // the contour the phase that finishes slot s bulk-loads the other chain's tile of slot s,
+    // forms the products in FP64 (exact for FP32 factors) and bulk-adds them into the FP64
+    // accumulator tile of the slot's block and the layout, in phase order.
+    const int co = 1 - c;
+    double* acc_unit = fphi ? a.phi_acc + (size_t)c * 4 * M + (size_t)p * PLANE : nullptr;
+    auto x_active = [&](int k) -> bool {
+        const long long s = slot0 + (long long)dir * k, kq = (s - a.slot0[co]) * a.dir[co];
+        return fphi && k >= 1 && k <= U && kq >= 1 && kq <= k - 2 && ((k - kq) & 1) == 0 && s != a.NsA;
+    };
+    unsigned xpar = 0, x_seen = 0;
+    bool x_pend = false;
 
     if (threadIdx.x == 0) {
         s_fail = 0;
         mbar_init(&s_bar, 1);
+        mbar_init(&s_xbar, 1);
         fence_mbar_init();
     }
     __syncthreads();
@@ -458,9 +480,13 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel_f32(con
         cp_async_wait_all();
         __syncthreads();
         if (s_fail) {
+            if (x_pend) mbar_wait(&s_xbar, xpar, kDrainSpins);
             if (warp == 0) bulk_wait_all();
             return;
         }
+        const long long s_fin = slot0 + (long long)dir * k;
+        const long long kp = (s_fin - a.slot0[co]) * a.dir[co];
+        const bool xact = x_active(k);
         float* cur = T0;
         float* oth = T1;
         if (k >= 1) {
@@ -485,6 +511,24 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel_f32(con
             if (threadIdx.x == 0) {
                 tma_store_5d(&a.tm_pq[c][plane ? 0 : 1], QS, 0, 0, 0, p, (int)(slot0 + (long long)dir * k));
                 bulk_commit();
+                if (xact) {  // XF was last read by the previous product pass (block barriers since)
+                    const unsigned* df = a.done + (size_t)co * N + p;
+                    long long spins = 0;
+                    while (x_seen < (unsigned)(kp + 1)) {
+                        x_seen = ld_acquire_u32(df);
+                        if (x_seen >= (unsigned)(kp + 1)) break;
+                        if (++spins > a.spin_limit) break;
+                        if (spins > 64) __nanosleep(32);
+                    }
+                    if (spins > a.spin_limit) {
+                        atomicOr(a.error, 32);
+                        s_fail = 1;  // no load issued; the block leaves after the next barrier
+                    } else {
+                        fence_async_global();
+                        mbar_expect_tx(&s_xbar, TILE_BYTES);
+                        tma_load_5d(XF, &a.tm_pq[co][plane ? 0 : 1], 0, 0, 0, p, (int)s_fin, &s_xbar);
+                    }
+                }
             }
         } else {
             tile_scale_f32<N, LF>(cur, Wl + blk_of(0) * S::WT);
@@ -501,12 +545,56 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel_f32(con
                 col_op_f32<N, N, LF, EO, kToGlobal>(cur, xo, sops);
             }
             __syncthreads();
+            if (xact && s_fail) {  // thread 0 gave up on the other chain's store: no load in flight
+                if (warp == 0) bulk_wait_all();
+                return;
+            }
             if (threadIdx.x < N) {  // tell consumer threadIdx.x that tile p of phase k is out
                 __threadfence();
                 st_release_u32((plane ? fl_plane : fl_slab) + (size_t)threadIdx.x * N + p, (unsigned)(k + 1));
             }
+            if (fphi && threadIdx.x == 0 && 2 * k == U) {  // the stores before the midpoint have landed
+                bulk_wait_but_newest();
+                fence_async_global();
+                st_release_u32(a.done + (size_t)c * N + p, (unsigned)k);
+            }
         }
-        __syncthreads();
+        if (fphi && k == 0) {  // zero the accumulator tiles, long before the first bulk add
+            for (int t4 = 0; t4 < 4; ++t4)
+                for (int i = threadIdx.x; i < N * N; i += kContourThreads) acc_unit[(size_t)t4 * M + i] = 0.0;
+            fence_async_global();
+        }
+        if (xact) {
+            if (threadIdx.x == 0) bulk_wait_read();  // the last bulk add has read PD
+            if (mbar_wait(&s_xbar, xpar, a.spin_limit)) {
+                xpar ^= 1u;
+            } else {
+                x_pend = true;
+                s_fail = 1;
+                atomicOr(a.error, 2);
+            }
+            __syncthreads();
+            if (s_fail) {
+                if (x_pend) mbar_wait(&s_xbar, xpar, kDrainSpins);
+                if (warp == 0) bulk_wait_all();
+                return;
+            }
+            for (int i = 2 * threadIdx.x; i < N * N; i += 2 * kContourThreads) {
+                const float2 v = *reinterpret_cast<const float2*>(QS + i);
+                const float2 w = *reinterpret_cast<const float2*>(XF + i);
+                *reinterpret_cast<double2*>(PD + i) = make_double2((double)v.x * w.x, (double)v.y * w.y);
+            }
+            fence_async_smem();
+            __syncthreads();  // also ends the phase
+            if (threadIdx.x == 0) {
+                bulk_wait_newest3();  // the add into this tile two phases back has completed
+                bulk_reduce_add_f64(acc_unit + (size_t)((s_fin < a.NsA ? 0 : 2) + (plane ? 0 : 1)) * M, PD,
+                                    N * N * (unsigned)sizeof(double));
+                bulk_commit();
+            }
+        } else {
+            __syncthreads();
+        }
     }
     if (warp == 0) bulk_wait_all();
 }

@@ -196,8 +196,9 @@ __global__ void phi_kernel(const T* __restrict__ q, const T* __restrict__ qc, do
 // (src/crysSCFT_sample.cpp:348-360: 1/2 at both ends of each block, 1 inside).  The panel
 // element of grid point (x, y, z) is (z / 8) * 8n + row * 8 + z % 8, with row y in plane
 // tile x and row x in slab tile y.
-__global__ void phi_fused_finish_kernel(const double* __restrict__ acc, const double* __restrict__ q,
-                                        const double* __restrict__ qc, double* __restrict__ phiA,
+template <typename T>
+__global__ void phi_fused_finish_kernel(const double* __restrict__ acc, const T* __restrict__ q,
+                                        const T* __restrict__ qc, double* __restrict__ phiA,
                                         double* __restrict__ phiB, const IterState* st, double fA, long long NsA,
                                         long long NsB, int n) {
     const long long n2 = (long long)n * n, M = n2 * n, U = NsA + NsB;
@@ -222,7 +223,7 @@ __global__ void phi_fused_finish_kernel(const double* __restrict__ acc, const do
         }
         for (int j = 0; j < nsp; ++j) {
             const long long s = sp[j];
-            const double w = q[s * M + i] * qc[s * M + i];
+            const double w = (double)q[s * M + i] * (double)qc[s * M + i];
             if (s <= NsA) a += (s == 0 || s == NsA ? 0.5 : 1.0) * w;
             if (s >= NsA) b += (s == NsA || s == U ? 0.5 : 1.0) * w;
         }

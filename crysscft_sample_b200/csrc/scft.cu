@@ -1031,7 +1031,8 @@ struct scft_diblock_s {
     DevBuf<double> d_xch;                 // exchange buffers, 2 x space_size_phy per chain
     DevBuf<unsigned> flags;               // per-unit phase flags of the alternating kernel
     bool fused_phi = true;                // FP64 alternating kernel sums phi itself (scft_diblock_set_phi_form)
-    bool phi_fused = false;               // the last launch_contour ran with the fused phi sums
+    bool phi_fused = false;               // the last launch_contour[_f32] ran with the fused phi sums
+    bool f32_phi_fused = false;           // the FP32 launch plan has room for them (setup_persistent_f32)
     DevBuf<double> phi_acc;               // its sums: [chain][block][layout][tile][n^2], 8 x space_size_phy
     int last_iter_precision = -1;         // precision of the iteration whose contour is stored
     DevBuf<double> stress_buf;            // batched temporaries of scft_diblock_stress
@@ -1136,6 +1137,7 @@ struct scft_diblock_s {
 
     int setup_persistent_f32() {
         persistent = false;
+        f32_phi_fused = false;
         CKR(setup_cluster_f32());
         if (cluster_f32) return SCFT_OK;
         const OpsSet* o = solver->ops;
@@ -1149,6 +1151,11 @@ struct scft_diblock_s {
         CK(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, solver->device));
         CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, solver->device));
         if (smem > (size_t)dev_smem) return SCFT_OK;
+        // fused phi sums: two more tiles (the other chain's FP32 tile, the FP64 products)
+        // where they fit (AltShapeF::SMEM_FUSED)
+        const size_t smem_fused = smem + (size_t)nx * nx * (sizeof(float) + sizeof(double));
+        f32_phi_fused = fused_phi && U % 2 == 0 && NsA >= 1 && NsB >= 1 && smem_fused <= (size_t)dev_smem;
+        if (f32_phi_fused) smem = smem_fused;
         CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 0;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, kContourThreads, smem));
@@ -1169,6 +1176,7 @@ struct scft_diblock_s {
     }
 
     int launch_contour_f32(cudaStream_t st, float* wAds, float* wBds, float* q, float* qc) {
+        phi_fused = false;
         if (cluster_f32) return launch_cluster_f32(st, wAds, wBds, q, qc);
         ContourArgsF a{};
         a.q[0] = q;
@@ -1189,6 +1197,12 @@ struct scft_diblock_s {
         a.spin_limit = spin_limit;
         a.flags = flags.p;
         const int n = (int)solver->grid_phy[0];
+        phi_fused = f32_phi_fused;  // set up with the launch's shared memory size
+        if (phi_fused) {
+            if (phi_acc.n != 8 * M) CKR(phi_acc.alloc(8 * M));
+            a.phi_acc = phi_acc.p;
+            a.done = flags.p + 4 * (size_t)n * n;
+        }
         for (int v = 0; v < 2; ++v) {  // panel tiles, plane [0] and slab [1] views
             CKR(encode_panel_map(&a.tm_pq[0][v], q, n, (long long)U + 1, v == 0, false));
             CKR(encode_panel_map(&a.tm_pq[1][v], qc, n, (long long)U + 1, v == 0, false));
@@ -1349,6 +1363,7 @@ struct scft_diblock_s {
                     fused = phi_fused;
                 } else {
                     CKR(launch_contour_f32(st, wAds, wBds, q, qc));
+                    fused = phi_fused;
                 }
                 ++solver->launches;
             }
@@ -1375,13 +1390,11 @@ struct scft_diblock_s {
         const int rblocks = (int)std::min<long long>(kRedMaxBlocks, (MM + kRedThreads - 1) / kRedThreads);
         q_reduce_kernel<T><<<rblocks, kRedThreads, 0, st>>>(qc, MM, partials.p, state.p);
         CK(cudaGetLastError());
-        if constexpr (sizeof(T) == 8) {
-            if (fused)
-                phi_fused_finish_kernel<<<grid_blocks(MM, 256), 256, 0, st>>>(
-                    phi_acc.p, q, qc, phiA.p, phiB.p, state.p, fA, (long long)NsA, (long long)NsB,
-                    (int)solver->grid_phy[0]);
-        }
-        if (!fused)
+        if (fused)
+            phi_fused_finish_kernel<T><<<grid_blocks(MM, 256), 256, 0, st>>>(
+                phi_acc.p, q, qc, phiA.p, phiB.p, state.p, fA, (long long)NsA, (long long)NsB,
+                (int)solver->grid_phy[0]);
+        else
             phi_kernel<T><<<grid_blocks((MM + 1) / 2, 256), 256, 0, st>>>(q, qc, phiA.p, phiB.p, state.p, fA,
                                                                           (long long)NsA, (long long)NsB, MM);
         CK(cudaGetLastError());

@@ -5,8 +5,9 @@ The alternating kernel adds q(s) q+(s) for the slots of the contour's second hal
 second chain reaches them; a short kernel adds slots 0, NsA, U/2 and U with their
 trapezoid weights.  Both forms must give the same free energy and phi up to the order of
 the sums.  The cases put the block boundary NsA below, at and above the midpoint U/2, run
-the bench system (64^3 physical, Ns = 200), a one-level P1 grid and an odd step count
-(the fused form is off there and the separate pass runs).  The reference parity of the
+the bench system (64^3 physical, Ns = 200), a one-level P1 grid, an odd step count (the
+fused form is off there and the separate pass runs) and the FP32 contour kernel of the
+precision form (FP32 tiles, FP64 products and sums).  The reference parity of the
 default (fused) form is the iteration tests' job.
 """
 import numpy as np
@@ -20,21 +21,26 @@ F_RTOL = 1e-13
 PHI_ATOL = 1e-13
 
 CASES = [
-    # kind, full grid, fA, ds, iterations: NsA / NsB
-    ("PMMM", (128, 128, 128), 0.25, 0.005, 3),  # 50 / 150, the bench system
-    ("PMMM", (32, 32, 32), 0.5, 0.01, 4),  # 50 / 50: NsA = U / 2
-    ("PMMM", (32, 32, 32), 0.7, 0.01, 4),  # 70 / 30: NsA above the midpoint
-    ("P1", (32, 32, 32), 0.25, 0.01, 4),  # one-level operators
-    ("PMMM", (64, 64, 64), 0.3, 0.0102, 4),  # 29 / 68: U odd, separate pass either way
+    # kind, full grid, fA, ds, iterations, precision of the triplets: NsA / NsB
+    ("PMMM", (128, 128, 128), 0.25, 0.005, 3, "fp64"),  # 50 / 150, the bench system
+    ("PMMM", (32, 32, 32), 0.5, 0.01, 4, "fp64"),  # 50 / 50: NsA = U / 2
+    ("PMMM", (32, 32, 32), 0.7, 0.01, 4, "fp64"),  # 70 / 30: NsA above the midpoint
+    ("P1", (32, 32, 32), 0.25, 0.01, 4, "fp64"),  # one-level operators
+    ("PMMM", (64, 64, 64), 0.3, 0.0102, 4, "fp64"),  # 29 / 68: U odd, separate pass either way
+    # FP32 contour kernel: FP32 tiles, products and sums in FP64
+    ("PMMM", (128, 128, 128), 0.25, 0.005, 3, "fp32"),
+    ("PMMM", (64, 64, 64), 0.5, 0.01, 3, "fp32"),
+    ("PMMM", (64, 64, 64), 0.7, 0.01, 3, "fp32"),
 ]
 
 
-def _run(kind, N, fA, ds, nit, fused):
+def _run(kind, N, fA, ds, nit, fused, precision="fp64"):
     L = 4.2
     wA, wB = fields.seed_fields(N, L, "BCC")
     G = solvers.make_solver(kind, N)
     G.set_cell_para((L, L, L))
     run = scft.DiblockSCFT(G, fA, ds, 20.0, 0.1)
+    run.set_precision(precision)
     run.set_phi_form(fused)
     run.set_fields(fields.to_physical(kind, wA), fields.to_physical(kind, wB))
     h = run.iterate(nit)
@@ -44,10 +50,10 @@ def _run(kind, N, fA, ds, nit, fused):
     return h
 
 
-@pytest.mark.parametrize("kind,N,fA,ds,nit", CASES)
-def test_fused_phi_matches_separate_pass(gpu, kind, N, fA, ds, nit):
-    a = _run(kind, N, fA, ds, nit, True)
-    b = _run(kind, N, fA, ds, nit, False)
+@pytest.mark.parametrize("kind,N,fA,ds,nit,precision", CASES)
+def test_fused_phi_matches_separate_pass(gpu, kind, N, fA, ds, nit, precision):
+    a = _run(kind, N, fA, ds, nit, True, precision)
+    b = _run(kind, N, fA, ds, nit, False, precision)
     rel = np.abs(a["F"] - b["F"]) / np.abs(b["F"])
     assert rel.max() <= F_RTOL, f"F rel diff {rel.max():.2e}"
     for k in ("phiA", "phiB"):
