@@ -1220,14 +1220,16 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
             __syncthreads();
         }
         if (k < U) {
-            if (warp == 0) issue_w(k + 1);  // W0/W1 are free: prefetch the next phase's factors
+            // W0/W1 are free: prefetch the next phase's factors (in a phase with the fused phi
+            // sums after them, so the bulk copies the sums wait for go first)
+            if (warp == 0 && !xact) issue_w(k + 1);
             // start step k on this layout with its column axis; the epilogue writes the
             // exchange buffer, which the other layout finishes (A_z, then its own axis) next phase
             const ColOut xo{(plane ? XP : XS) + off, gs};
             col_global(cur, xo, plane ? OFFY : 0);
             __syncthreads();
             if (xact && s_fail) {  // thread 0 gave up on the other chain's store: no load in flight
-                drain(true);
+                drain(false);
                 return;
             }
             if (threadIdx.x < N) {  // tell consumer threadIdx.x that tile p of phase k is out
@@ -1259,8 +1261,8 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
                 atomicOr(a.error, 2);
             }
             __syncthreads();
-            if (s_fail) {
-                drain(k < U);
+            if (s_fail) {  // the next phase's factors are not requested yet
+                drain(false);
                 return;
             }
             // QS <- q(s) q+(s), then one bulk add into the accumulator tile; the next phase's
@@ -1284,6 +1286,7 @@ __global__ void __launch_bounds__(kContourThreads, 1) contour_alt_kernel(const _
                                     TILE_BYTES);
                 bulk_commit();
             }
+            if (warp == 0) issue_w(k + 1);  // an active phase is never the last (kp >= 1)
         } else {
             __syncthreads();
             if (fphi && s_fail) {
